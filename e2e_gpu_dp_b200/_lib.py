@@ -1,0 +1,119 @@
+"""ctypes binding of the C ABI in include/e2e_dp.h (libe2edp.so, built in-tree).
+
+The library is the only compute path: if it is missing the import fails
+loudly; there is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import threading
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libe2edp.so")
+
+E2E_OK = 0
+E2E_HOST, E2E_DEVICE = 0, 1
+E2E_COUNT_U16, E2E_COUNT_U32, E2E_VALUE_F32, E2E_COUNT_AUTO = 0, 1, 2, -1
+
+STATUS = {
+    0: "E2E_OK", 1: "E2E_ERR_INVALID", 2: "E2E_ERR_CUDA", 3: "E2E_ERR_NOMEM", 4: "E2E_ERR_IO",
+    5: "E2E_ERR_TIMEOUT", 6: "E2E_ERR_NOT_CONVERGED", 7: "E2E_ERR_UNSUPPORTED",
+    8: "E2E_ERR_DEVICE", 9: "E2E_ERR_CANCELLED", 10: "E2E_ERR_BUSY",
+}
+
+
+class E2EError(RuntimeError):
+    def __init__(self, status: int, msg: str):
+        super().__init__(f"{STATUS.get(status, status)}: {msg}")
+        self.status = status
+
+
+class Problem(C.Structure):
+    _fields_ = [
+        ("gsize", C.c_int32), ("num_actions", C.c_int32), ("nrzns", C.c_int32), ("F", C.c_float),
+        ("dt", C.c_float), ("r_outbound", C.c_float), ("r_terminal", C.c_float),
+        ("nmodes", C.c_int32), ("i_term", C.c_int32), ("j_term", C.c_int32), ("nt", C.c_int32),
+        ("is_stationary", C.c_int32), ("term_subgrid_size", C.c_int32),
+        ("reward_type", C.c_int32), ("num_ac_speeds", C.c_int32), ("num_ac_angles", C.c_int32),
+        ("dx", C.c_float), ("dy", C.c_float), ("neighb_gsize", C.c_int32), ("alpha", C.c_float),
+        ("x0", C.c_float), ("y0", C.c_float),
+    ]
+
+
+class Fields(C.Structure):
+    _fields_ = [(n, C.c_void_p) for n in ("u", "v", "ui", "vi", "yi", "s", "mask")]
+
+
+class BuildOpts(C.Structure):
+    _fields_ = [("count_type", C.c_int32), ("tile_cells", C.c_int32), ("stage_hint", C.c_int64),
+                ("keep_reward_parts", C.c_int32), ("reserved", C.c_int32)]
+
+
+class ModelInfo(C.Structure):
+    _fields_ = [
+        ("ns", C.c_int64), ("n_rows", C.c_int64), ("nnz", C.c_int64), ("num_actions", C.c_int32),
+        ("nt", C.c_int32), ("ncells", C.c_int32), ("nrzns", C.c_int32), ("count_type", C.c_int32),
+        ("index_bits", C.c_int32), ("row_ptr", C.c_void_p), ("col", C.c_void_p),
+        ("cnt", C.c_void_p), ("R", C.c_void_p), ("dropped", C.c_uint64),
+        ("overflow_units", C.c_uint64),
+    ]
+
+
+class ViOpts(C.Structure):
+    _fields_ = [("method", C.c_int32), ("threshold", C.c_float), ("max_iter", C.c_int32),
+                ("timeout_s", C.c_double), ("fp64_check", C.c_int32), ("reserved", C.c_int32)]
+
+
+class ViStats(C.Structure):
+    _fields_ = [("iterations", C.c_int32), ("residual", C.c_double), ("seconds", C.c_double),
+                ("fp64_max_abs_err", C.c_double), ("fp64_max_rel_err", C.c_double),
+                ("bytes_per_sweep", C.c_int64)]
+
+
+# every exported symbol of include/e2e_dp.h with its signature
+SIGNATURES = {
+    "e2e_abi_version": (C.c_int, []),
+    "e2e_status_string": (C.c_char_p, [C.c_int]),
+    "e2e_last_error": (C.c_char_p, []),
+    "e2e_problem_from_params": (C.c_int, [C.POINTER(C.c_float), C.POINTER(Problem)]),
+    "e2e_problem_to_params": (C.c_int, [C.POINTER(Problem), C.POINTER(C.c_float)]),
+    "e2e_action_table": (C.c_int, [C.POINTER(Problem)] + [C.POINTER(C.c_float)] * 4),
+    "e2e_build_model": (C.c_int, [C.POINTER(Problem), C.POINTER(Fields), C.c_int,
+                                  C.POINTER(BuildOpts), C.POINTER(C.c_void_p), C.c_void_p]),
+    "e2e_model_free": (C.c_int, [C.c_void_p]),
+    "e2e_model_get_info": (C.c_int, [C.c_void_p, C.POINTER(ModelInfo)]),
+    "e2e_model_copy_to_host": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                         C.c_void_p, C.c_void_p]),
+    "e2e_model_write_npy": (C.c_int, [C.c_void_p, C.POINTER(Problem), C.c_char_p, C.c_int]),
+    "e2e_model_read_npy": (C.c_int, [C.c_char_p, C.POINTER(C.c_void_p), C.c_void_p]),
+    "e2e_spvi_solve": (C.c_int, [C.c_void_p, C.POINTER(ViOpts), C.c_void_p, C.c_void_p, C.c_int,
+                                 C.POINTER(ViStats), C.c_void_p]),
+}
+
+_lib = None
+_lock = threading.Lock()
+
+
+def lib():
+    """Load libe2edp.so (fails loudly if it was not built)."""
+    global _lib
+    with _lock:
+        if _lib is None:
+            if not os.path.exists(LIB_PATH):
+                raise ImportError(
+                    f"{LIB_PATH} is missing: build it with `make -C e2e_gpu_dp_b200/csrc` "
+                    "(there is no CPU fallback)")
+            L = C.CDLL(LIB_PATH)
+            for name, (res, args) in SIGNATURES.items():
+                fn = getattr(L, name)
+                fn.restype = res
+                fn.argtypes = args
+            _lib = L
+    return _lib
+
+
+def check(status: int) -> None:
+    if status != E2E_OK:
+        msg = lib().e2e_last_error()
+        raise E2EError(status, msg.decode() if msg else "")

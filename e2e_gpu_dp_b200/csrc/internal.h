@@ -1,0 +1,79 @@
+// Host-side internals shared by the C ABI translation units.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <string>
+#include <vector>
+
+#include "e2e_dp.h"
+#include "kernels.h"
+
+// The model handle behind the opaque e2e_model of the public header.
+struct e2e_model {
+  int64_t ns = 0;            // states
+  int64_t n_rows = 0;        // rows (s, a) stored: n_row_states * na
+  int64_t n_row_states = 0;  // states that own rows; later states have Q = R only
+  int64_t nnz = 0;
+  int32_t na = 0, nt = 0, ncells = 0, nrzns = 1;
+  int32_t count_type = E2E_COUNT_U16;
+  int32_t index_bits = 32;
+  void* row_ptr = nullptr;   // device
+  int32_t* col = nullptr;    // device
+  void* cnt = nullptr;       // device
+  float* R = nullptr;        // device, ns * na (state-major)
+  uint64_t dropped = 0, misbinned = 0, overflow_rows = 0;
+  bool layered = false;      // every transition of a layer-t state leads into layer t+1
+  e2e_problem prob{};
+  bool has_prob = false;
+};
+
+namespace e2e {
+
+e2e_status fail(e2e_status st, const std::string& msg);
+e2e_status cuda_fail(cudaError_t e, const char* what);
+
+// Stream-ordered temporaries released when the owner goes out of scope.
+struct DeviceScratch {
+  cudaStream_t st;
+  std::vector<void*> ptrs;
+  explicit DeviceScratch(cudaStream_t s) : st(s) {}
+  void add(void* p) {
+    if (p) ptrs.push_back(p);
+  }
+  ~DeviceScratch() {
+    for (void* p : ptrs) cudaFreeAsync(p, st);
+  }
+  DeviceScratch(const DeviceScratch&) = delete;
+  DeviceScratch& operator=(const DeviceScratch&) = delete;
+};
+
+struct BuildPlan {
+  int count_bits = 16;
+  int64_t ncells = 0, ns = 0, n_rows = 0, tiles_per_layer = 0, n_tiles = 0;
+  int na = 0, rc = 128;
+  int64_t stage_cap = 0, pool_units = 0;
+};
+
+struct FieldsOnDevice {
+  DevFields F{};
+  size_t h2d_bytes = 0;
+};
+
+e2e_status validate_problem(const e2e_problem* p);
+void host_ticks(const e2e_problem* p, std::vector<float>& xs, std::vector<float>& ys);
+void host_actions(const e2e_problem* p, std::vector<float>& speed, std::vector<float>& angle);
+e2e_status make_dev_problem(const e2e_problem* p, cudaStream_t st, DevProblem* D,
+                            DeviceScratch* keep);
+e2e_status plan_build(const e2e_problem* p, int count_bits, int64_t stage_hint, BuildPlan* pl);
+e2e_status fields_to_device(const e2e_problem* p, const e2e_fields* f, int where, cudaStream_t st,
+                            FieldsOnDevice* fd, DeviceScratch* keep);
+e2e_status run_build(const e2e_problem* p, const DevFields& F, const BuildPlan& pl,
+                     cudaStream_t st, DeviceScratch* scratch, e2e_model* m);
+ViModel vi_model(const e2e_model* m);
+void free_model_buffers(e2e_model* m);
+int64_t model_bytes(const e2e_model* m);
+e2e_status solve_on_device(const e2e_model* m, const e2e_vi_opts& o, float* dV, int32_t* dpi,
+                           e2e_vi_stats* stats, cudaStream_t st);
+
+}  // namespace e2e

@@ -1,0 +1,204 @@
+/*
+ * e2e_dp.h -- C ABI of the B200 end-to-end dynamic-programming planner:
+ * Monte-Carlo transition build -> CSR assembly -> sparse value iteration.
+ *
+ * The reference (rohit1607/e2e_GPU_DP) has no library API: its boundary is two
+ * executables, src/build_model.cu (main :926) and src/spvi_2.cu (main :730),
+ * that exchange .npy files.  Each entry point below names the reference
+ * function or file-protocol step it replaces.  The drop-in executables
+ * `build_model` and `spvi_2` of this package are thin C++ mains over this ABI
+ * that keep the reference's command line and file layout.
+ *
+ * Conventions
+ *  - Plain C types only; every function returns an e2e_status and never aborts.
+ *  - `stream` is a cudaStream_t passed as void* (NULL = the legacy default stream).
+ *  - `where` arguments say whether a pointer is host (E2E_HOST) or device (E2E_DEVICE)
+ *    memory of the current CUDA device.
+ *  - A model handle is owned by the caller and released with e2e_model_free().
+ *    Handles are independent (no global state), so different host threads may
+ *    work on different handles; one handle must not be used by two threads at once.
+ *  - Indices: state s = t*ncells + i*gsize + j (src/build_model.cu:81-91); model row
+ *    (s, a) has index s*num_actions + a ("state-major").  The reference's on-disk COO
+ *    is action-major (row a*Ns + s); e2e_model_write_npy/e2e_model_read_npy convert.
+ */
+#ifndef E2E_DP_H
+#define E2E_DP_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define E2E_DP_ABI_VERSION 1
+
+typedef enum {
+  E2E_OK = 0,
+  E2E_ERR_INVALID = 1,       /* bad argument or problem definition */
+  E2E_ERR_CUDA = 2,          /* a CUDA runtime call failed (see e2e_last_error) */
+  E2E_ERR_NOMEM = 3,         /* device or host allocation failed */
+  E2E_ERR_IO = 4,            /* .npy read/write failed or a file is malformed */
+  E2E_ERR_TIMEOUT = 5,       /* host wall-clock limit reached */
+  E2E_ERR_NOT_CONVERGED = 6, /* max_iter reached before the threshold */
+  E2E_ERR_UNSUPPORTED = 7,   /* valid input outside what this build implements */
+  E2E_ERR_DEVICE = 8,        /* a device-side check failed (bounded wait, pool, overflow) */
+  E2E_ERR_CANCELLED = 9,     /* request cancelled (server) */
+  E2E_ERR_BUSY = 10          /* admission refused: not enough free device memory (server) */
+} e2e_status;
+
+enum { E2E_HOST = 0, E2E_DEVICE = 1 };
+
+/* Count storage of a model: exact integer counts scaled by 1/nrzns, or plain
+ * float probabilities (models read from arbitrary COO files). */
+enum { E2E_COUNT_U16 = 0, E2E_COUNT_U32 = 1, E2E_VALUE_F32 = 2, E2E_COUNT_AUTO = -1 };
+
+/*
+ * Problem definition.  Fields 0..19 are the slots of the reference's 32-float
+ * `prob_params` vector in slot order (src/build_model.cu:1032-1055, saved as
+ * prob_params.npy at :1310); x0/y0 are the grid origin (header: x0 = dx/2,
+ * src/input_to_build_model.h:14-15).  reward_type: 0 time, 1 energy1,
+ * 2 energy2, 3 energy3, 4 custom1 (get_reward_type, src/build_model.cu:898-918).
+ */
+typedef struct {
+  int32_t gsize;             /* 0 */
+  int32_t num_actions;       /* 1 = num_ac_speeds * num_ac_angles */
+  int32_t nrzns;             /* 2 */
+  float F;                   /* 3 max vehicle speed */
+  float dt;                  /* 4 */
+  float r_outbound;          /* 5 */
+  float r_terminal;          /* 6 */
+  int32_t nmodes;            /* 7 */
+  int32_t i_term;            /* 8 */
+  int32_t j_term;            /* 9 */
+  int32_t nt;                /* 10 */
+  int32_t is_stationary;     /* 11 (unused by the kernels, as in the reference) */
+  int32_t term_subgrid_size; /* 12 */
+  int32_t reward_type;       /* 13 */
+  int32_t num_ac_speeds;     /* 14 */
+  int32_t num_ac_angles;     /* 15 */
+  float dx;                  /* 16 */
+  float dy;                  /* 17 */
+  int32_t neighb_gsize;      /* 18 (m, odd, <= gsize) */
+  float alpha;               /* 19 */
+  float x0;                  /* grid origin, cell (.., j) centre x = x0 + j*dx */
+  float y0;
+} e2e_problem;
+
+/*
+ * Input fields in the reference's layout and dtypes (src/build_model.cu:978-1019):
+ * u, v, s, mask: (nt, gsize, gsize); ui, vi: (nt, nmodes, gsize, gsize);
+ * yi: (nt, nrzns, nmodes).  float32 except mask (int32; 1 = obstacle).
+ */
+typedef struct {
+  const float* u;
+  const float* v;
+  const float* ui;
+  const float* vi;
+  const float* yi;
+  const float* s;
+  const int32_t* mask;
+} e2e_fields;
+
+typedef struct {
+  int32_t count_type;   /* E2E_COUNT_AUTO (u16 when nrzns < 65536), E2E_COUNT_U16 or _U32 */
+  int32_t tile_cells;   /* 0 = default (32); cells per builder tile, multiple of 32 */
+  int64_t stage_hint;   /* 0 = default; initial staging capacity in entries */
+  int32_t keep_reward_parts; /* 1: also keep per-entry reward sums for target re-use (server) */
+  int32_t reserved;
+} e2e_build_opts;
+
+typedef struct {
+  int64_t ns;            /* states = nt * gsize^2 */
+  int64_t n_rows;        /* rows with transitions = (nt-1) * gsize^2 * num_actions */
+  int64_t nnz;
+  int32_t num_actions;
+  int32_t nt;
+  int32_t ncells;
+  int32_t nrzns;         /* count scale (1 for E2E_VALUE_F32 models) */
+  int32_t count_type;    /* E2E_COUNT_U16, _U32 or E2E_VALUE_F32 */
+  int32_t index_bits;    /* 32 or 64: width of row_ptr */
+  const void* row_ptr;   /* device, n_rows + 1 (int32 or int64) */
+  const int32_t* col;    /* device, nnz: absolute next state S2 */
+  const void* cnt;       /* device, nnz: uint16 / uint32 counts or float values */
+  const float* R;        /* device, ns * num_actions, state-major */
+  uint64_t dropped;      /* samples outside the m x m neighbourhood (not counted, as the reference's bin m*m) */
+  uint64_t overflow_units; /* rows whose samples spread beyond the builder's fast window */
+} e2e_model_info;
+
+typedef struct e2e_model e2e_model;
+
+typedef struct {
+  int32_t method;        /* 0 = Jacobi sweeps from V=0 (reference semantics),
+                            1 = layered backward sweep + one verification sweep */
+  float threshold;       /* Jacobi stop: sup-norm < threshold (reference default 0.1) */
+  int32_t max_iter;      /* 0 = nt + 2 */
+  double timeout_s;      /* host wall-clock limit, 0 = none */
+  int32_t fp64_check;    /* 1: FP64 backward solve on the device, report the error of the FP32 values */
+  int32_t reserved;
+} e2e_vi_opts;
+
+typedef struct {
+  int32_t iterations;      /* sweeps performed (layered: 1 + verification sweep) */
+  double residual;         /* last sup-norm |V' - V| (FP64 reduction) */
+  double seconds;          /* device time of the solve (CUDA events) */
+  double fp64_max_abs_err; /* fp64_check: max |V32 - V64| */
+  double fp64_max_rel_err; /* fp64_check: max |V32 - V64| / max |V64| */
+  int64_t bytes_per_sweep; /* algorithmic bytes of one sweep */
+} e2e_vi_stats;
+
+/* ---- library ------------------------------------------------------------ */
+int e2e_abi_version(void);
+const char* e2e_status_string(e2e_status st);
+/* Message of the last failure on the calling host thread ("" if none). */
+const char* e2e_last_error(void);
+
+/* prob_params.npy slots <-> e2e_problem (src/build_model.cu:1032-1055). */
+e2e_status e2e_problem_from_params(const float prob_params[32], e2e_problem* out);
+e2e_status e2e_problem_to_params(const e2e_problem* p, float prob_params_out[32]);
+
+/* Action table: speed and heading per action index j + num_ac_angles*i
+ * (populate_actions, src/build_model.cu:1438-1457) and their cosf/sinf as
+ * evaluated on the device (the builder's move(), src/build_model.cu:284-285). */
+e2e_status e2e_action_table(const e2e_problem* p, float* speed, float* angle, float* cosv,
+                            float* sinv);
+
+/* ---- build (replaces build_model main, src/build_model.cu:926-1238, and the
+ * per-(t,a) worker build_sparse_transition_model_at_T_at_a, :696-892) -------- */
+e2e_status e2e_build_model(const e2e_problem* p, const e2e_fields* fields, int fields_where,
+                           const e2e_build_opts* opts /* may be NULL */, e2e_model** out,
+                           void* stream);
+e2e_status e2e_model_free(e2e_model* m);
+e2e_status e2e_model_get_info(const e2e_model* m, e2e_model_info* info);
+
+/* Copy the CSR to host buffers (any may be NULL): row_ptr as int64 (n_rows+1),
+ * col (nnz), counts widened to uint32 (nnz; E2E_VALUE_F32 models: the float bits),
+ * R (ns*num_actions). */
+e2e_status e2e_model_copy_to_host(const e2e_model* m, int64_t* row_ptr, int32_t* col,
+                                  uint32_t* cnt, float* R, void* stream);
+
+/* Write the reference's model files into `dir` (save_master_Coos_to_file,
+ * src/build_model.cu:1246-1314): master_cooS1/S2 (int64, or int32 after the
+ * reference's convert step when index_bits == 32, src/convert_model_datatype.py:19-23),
+ * master_cooVal (f32 count/nrzns), master_R (f32, action-major), DP_relv_params
+ * (int64 [Ns, Na]) and prob_params (f32[32]). */
+e2e_status e2e_model_write_npy(const e2e_model* m, const e2e_problem* p, const char* dir,
+                               int index_bits);
+
+/* Load a model directory in the reference layout (get_mdp_model,
+ * src/spvi_2.cu:393-504): S1/S2 int32 or int64, Val f32, R f32, DP_relv_params.
+ * If prob_params.npy is present and every value is count/nrzns, the model is
+ * stored as exact counts; otherwise as float values. */
+e2e_status e2e_model_read_npy(const char* dir, e2e_model** out, void* stream);
+
+/* ---- solve (replaces solver_spvi_solve, src/spvi_2.cu:650-726, with the
+ * backup of solver_do_backup :174-260, select_best_action :93-122 and
+ * compute_sup_norm :263-356 fused into one kernel per sweep) ----------------- */
+e2e_status e2e_spvi_solve(const e2e_model* m, const e2e_vi_opts* opts /* may be NULL */,
+                          int32_t* policy_out, float* value_out, int out_where,
+                          e2e_vi_stats* stats /* may be NULL */, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* E2E_DP_H */
