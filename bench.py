@@ -1,0 +1,445 @@
+"""Benchmark: end-to-end planner (Monte-Carlo build + value iteration) on one B200.
+
+One step = build the transition model of the single-large-solve workload
+(200x200 grid, nt=120, 16 headings, 5000 realisations, 10 modes) and solve it
+(layered backward sweep + one FP64-residual verification sweep).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Prints one JSON line (rank 0).  `value` is seconds per solve with the fields
+already resident in HBM; `e2e` is the same through the C ABI from pinned host
+buffers (fields host->device and value/policy device->host inside the timed
+region).  Extra keys: the fused VI sweep's bandwidth, the dominant kernel's
+roofline, the CPU baseline (the oracle port on the host cores) and clocks.
+The reference arm runs the reference's own build_model -> convert -> spvi_2
+(compiled from its sources into oracle/_ref) on the same workload.
+Multi-GPU: independent replicas, one per rank (the workload does not shard).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOAD = "c2"
+PEAKS_FILE = os.path.join(ROOT, "MEASURED_PEAKS.json")
+FALLBACK_HBM_GBS = 6650.0
+
+
+def _peaks():
+    try:
+        with open(PEAKS_FILE) as fh:
+            d = json.load(fh)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+class Clocks:
+    """nvidia-smi sampler over the timed region (200 ms period)."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int):
+        self.dev = device_index
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        try:
+            import torch
+
+            uuid = str(torch.cuda.get_device_properties(self.dev).uuid)
+            sel = ["-i", "GPU-" + uuid if not uuid.startswith("GPU-") else uuid]
+        except Exception:
+            sel = ["-i", str(self.dev)]
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", *sel, f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+            time.sleep(0.3)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            time.sleep(0.25)
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.path or not os.path.exists(self.path):
+            return None
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        with open(self.path) as fh:
+            for line in fh:
+                parts = [p.strip() for p in line.split(",")]
+                if len(parts) < 9:
+                    continue
+                try:
+                    sm.append(float(parts[1]))
+                    smax.append(float(parts[2]))
+                except ValueError:
+                    continue
+                for n, v in zip(names, parts[5:9]):
+                    if v.lower().startswith("active"):
+                        reasons.add(n)
+        os.unlink(self.path)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(smax),
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def _dist():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+def _max_over_ranks(x: float, ws: int) -> float:
+    if ws == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def _barrier(ws):
+    if ws > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+
+
+def algorithmic_build_bytes(prob, nnz: int, count_bytes: int) -> int:
+    """Bytes the builder must move once: fields read once per layer (u, v, the
+    2*nmodes mode fields and the mask at t and t+1 per cell, the layer's Y
+    coefficients) and the model written (staged CSR entries, per-row offset and R)."""
+    nc, nt, nm = prob.ncells, prob.nt, prob.nmodes
+    layers = nt - 1
+    reads = layers * (nc * (2 + 2 * nm) * 4 + nc * 2 * 4 + prob.nrzns * nm * 4)
+    rows = layers * nc * prob.num_actions
+    writes = nnz * (4 + count_bytes) + rows * (4 + 4)
+    return int(reads + writes)
+
+
+def cpu_baseline(prob, fields, threads: int, target_s: float = 15.0):
+    """The oracle (C restatement) on a bounded sample of rows, extrapolated."""
+    from oracle import pyoracle as O
+
+    n_rows = (prob.nt - 1) * prob.ncells * prob.num_actions
+    # calibrate on a small block, then run a block sized for ~target_s
+    probe = 2048
+    t0 = time.perf_counter()
+    O.build_rows(prob, fields, r0=n_rows // 2, r1=n_rows // 2 + probe, nthreads=threads)
+    dt = time.perf_counter() - t0
+    rows = int(min(n_rows, max(probe, probe * target_s / max(dt, 1e-6))))
+    chunks = 8
+    per = max(1, rows // chunks)
+    t0 = time.perf_counter()
+    done = 0
+    nnz = 0
+    for c in range(chunks):
+        r0 = int((c + 0.5) * n_rows / chunks) - per // 2
+        out = O.build_rows(prob, fields, r0=r0, r1=r0 + per, nthreads=threads)
+        done += per
+        nnz += len(out["col"])
+    el = time.perf_counter() - t0
+    est_build = el * n_rows / done
+    # FP64 backward sweep: time on the sampled rows and scale by nnz
+    rp = out["row_ptr"]
+    t1 = time.perf_counter()
+    for _ in range(3):
+        acc = np.add.reduceat(out["cnt"].astype(np.float64) * 1e-3, rp[:-1][np.diff(rp) > 0])
+    vi_per_nnz = (time.perf_counter() - t1) / 3 / max(1, len(out["col"]))
+    est_nnz = nnz * n_rows / done
+    est_vi = vi_per_nnz * est_nnz
+    return {
+        "value": est_build + est_vi, "unit": "s", "cores": threads, "kind": "port",
+        "sample": f"oracle build of {done} of {n_rows} rows ({chunks} blocks spread over the layers) "
+                  f"in {el:.1f}s on {threads} threads, extrapolated linearly; VI one FP64 sweep "
+                  f"estimated from the sampled rows",
+    }
+
+
+def run_ours(args, ws, rank, local):
+    import torch
+
+    from e2e_gpu_dp_b200 import api
+    from e2e_gpu_dp_b200.problem import config, make_fields
+
+    torch.cuda.set_device(local)
+    prob, spec = config(WORKLOAD, seed=1234 + rank)
+    fields = make_fields(prob, spec)
+    dev = {k: torch.from_numpy(np.ascontiguousarray(v)).cuda() for k, v in fields.items()}
+    stream = torch.cuda.current_stream()
+    V = torch.empty(prob.ns, dtype=torch.float32, device="cuda")
+    pi = torch.empty(prob.ns, dtype=torch.int32, device="cuda")
+
+    def step(record=None):
+        m = api.build_model(prob, dev, stream=stream)
+        _, _, st = m.solve(method="layered", value=V, policy=pi, stream=stream)
+        if record is not None:
+            record.append((m.info(), st))
+        m.free()
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    _barrier(ws)
+    recs = []
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    with Clocks(local) as clk:
+        torch.cuda.synchronize()
+        e0.record(stream)
+        for _ in range(args.steps):
+            step(recs)
+        e1.record(stream)
+        torch.cuda.synchronize()
+    _barrier(ws)
+    ms = e0.elapsed_time(e1) / args.steps
+    ms = _max_over_ranks(ms, ws)
+    clocks = clk.summary()
+
+    info = recs[-1][0]
+    k1_ms = statistics.mean(r[0]["build_kernel_ms"] for r in recs)
+    asm_ms = statistics.mean(r[0]["assemble_ms"] for r in recs)
+    solve_ms = statistics.mean(r[1]["seconds"] * 1e3 for r in recs)
+    launches = 4 + (prob.nt + 1)  # trig, build, scan, assemble; last layer + nt-1 layers + verification
+
+    # e2e through the C ABI from pinned host memory
+    pinned = {k: torch.from_numpy(np.ascontiguousarray(v)).pin_memory() for k, v in fields.items()}
+    hV = torch.empty(prob.ns, dtype=torch.float32).pin_memory()
+    hpi = torch.empty(prob.ns, dtype=torch.int32).pin_memory()
+    host_fields = {k: t.numpy() for k, t in pinned.items()}
+    h2d = int(sum(t.numel() * t.element_size() for t in pinned.values()))
+    d2h = int(hV.numel() * 4 + hpi.numel() * 4)
+
+    def e2e_step():
+        m = api.build_model(prob, host_fields, stream=stream)
+        m.solve(method="layered", value=hV, policy=hpi, stream=stream)
+        m.free()
+
+    for _ in range(max(1, min(args.warmup, 2))):
+        e2e_step()
+    torch.cuda.synchronize()
+    _barrier(ws)
+    t0 = time.perf_counter()
+    f0 = torch.cuda.Event(enable_timing=True)
+    f1 = torch.cuda.Event(enable_timing=True)
+    f0.record(stream)
+    for _ in range(args.steps):
+        e2e_step()
+    f1.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = max(f0.elapsed_time(f1), (time.perf_counter() - t0) * 1e3) / args.steps
+    e2e_ms = _max_over_ranks(e2e_ms, ws)
+
+    # the fused VI kernel in the reference's Jacobi schedule (VI SpMV GB/s)
+    m = api.build_model(prob, dev, stream=stream)
+    _, _, jst = m.solve(method="jacobi", threshold=0.1, value=V, policy=pi, stream=stream)
+    _, _, lst = m.solve(method="layered", fp64_check=True, value=V, policy=pi, stream=stream)
+    m.free()
+    hbm, peak_kind = _peaks()
+    vi_gbs = jst["bytes_per_sweep"] * jst["iterations"] / jst["seconds"] / 1e9
+
+    cb = 2 if info["count_type"] == 0 else 4
+    k1_bytes = algorithmic_build_bytes(prob, info["nnz"], cb)
+    k1_gbs = k1_bytes / (k1_ms * 1e-3) / 1e9
+    traffic = None
+    tpath = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(tpath):
+        try:
+            traffic = json.load(open(tpath)).get(f"k_build_tiles/{WORKLOAD}")
+        except Exception:
+            traffic = None
+    samples = (prob.nt - 1) * prob.ncells * prob.num_actions * prob.nrzns
+
+    value_s = ms / 1e3 / ws
+    line = {
+        "metric": "build+VI sec",
+        "value": round(value_s, 6),
+        "unit": "s",
+        "n_gpus": ws,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": round(ms, 3),
+        "higher_is_better": False,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "fp32 values, u16 counts, fp64 residual",
+        "data": "synthetic (seeded double gyre + Fourier modes, reference layout)",
+        "config": {
+            "workload": "single large solve: 200x200 grid, nt=120, 16 headings, F=1, nrzns=5000, "
+                        "10 modes sigma_k=0.3/2^(k/2), gyre A=1, 3% obstacles",
+            "states": prob.ns, "rows": info["n_rows"], "nnz": info["nnz"], "samples": samples,
+            "solve": "layered backward sweep + FP64-residual verification sweep",
+            "parallelism": f"replicas x{ws}", "l2": "inputs (fields 0.45 GB, model 2.2 GB) exceed L2",
+        },
+        "e2e": {"value": round(e2e_ms / 1e3 / ws, 6), "unit": "s", "h2d_bytes_per_step": h2d,
+                "d2h_bytes_per_step": d2h},
+        "gpu_launches": launches,
+        "phases_ms": {"build_kernel": round(k1_ms, 3), "assemble": round(asm_ms, 3),
+                      "solve": round(solve_ms, 3)},
+        "roofline": {"kernel": "k_build_tiles", "bound": "hbm", "achieved": round(k1_gbs, 2),
+                     "peak": hbm, "unit": "GB/s", "frac": round(k1_gbs / hbm, 5),
+                     "traffic": traffic, "peak_source": f"{peak_kind} hbm_gbs",
+                     "algorithmic_bytes": k1_bytes,
+                     "note": "issue-bound Monte-Carlo kernel; samples/s is its throughput"},
+        "build_samples_per_s": round(samples / (k1_ms * 1e-3), 1),
+        "vi": {"kernel": "k_vi_sweep (Jacobi, reference schedule)", "iterations": jst["iterations"],
+               "bytes_per_sweep": jst["bytes_per_sweep"], "seconds": round(jst["seconds"], 6),
+               "achieved_gbs": round(vi_gbs, 1), "frac": round(vi_gbs / hbm, 4),
+               "layered_seconds": round(lst["seconds"], 6),
+               "fp64_max_rel_err": lst["fp64_max_rel_err"]},
+        "clocks": clocks,
+    }
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(prob, fields, threads=os.cpu_count() or 1)
+    return line
+
+
+def run_reference(args, ws, rank, local):
+    if rank != 0:
+        return None
+    from oracle import run_ref
+    from e2e_gpu_dp_b200.problem import config, make_fields
+
+    if not (run_ref.have_reference(WORKLOAD) and run_ref.have_reference("t_time")):
+        return {"impl": "reference", "unavailable": "reference binaries not built into oracle/_ref "
+                "(python oracle/build_ref.py needs the reference sources)"}
+    prob, spec = config(WORKLOAD, seed=1234)
+    fields = make_fields(prob, spec)
+    work = tempfile.mkdtemp(prefix="e2e_ref_")
+    try:
+        for _ in range(args.warmup):  # process start, driver and binary warm-up on a small problem
+            run_ref.run("t_time", os.path.join(work, "warm"), keep_model=False)
+        runs = []
+        with Clocks(local) as clk:
+            for _ in range(args.steps):
+                runs.append(run_ref.run(WORKLOAD, os.path.join(work, "c2"), prob=prob, fields=fields,
+                                        keep_model=False))
+        clocks = clk.summary()
+    finally:
+        subprocess.run(["rm", "-rf", work])
+    wall = [r["wall_build_s"] + r["wall_convert_s"] + r["wall_solve_s"] for r in runs]
+    value = statistics.mean(wall)
+    return {
+        "impl": "reference",
+        "metric": "build+VI sec",
+        "value": round(value, 4),
+        "unit": "s",
+        "n_gpus": 1,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": round(value * 1e3, 1),
+        "higher_is_better": False,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "fp32",
+        "data": "synthetic (same seeded inputs as the ours arm)",
+        "config": {"workload": "single large solve: 200x200 grid, nt=120, 16 headings, F=1, "
+                               "nrzns=5000, 10 modes", "pipeline": "build_model -> convert -> spvi_2"},
+        "phases_s": {"build_loop": statistics.mean(r["build_loop_s"] for r in runs),
+                     "build_process": statistics.mean(r["wall_build_s"] for r in runs),
+                     "convert": statistics.mean(r["wall_convert_s"] for r in runs),
+                     "solve_process": statistics.mean(r["wall_solve_s"] for r in runs),
+                     "solve_total_reported": statistics.mean(r["solve_total_s"] or 0 for r in runs),
+                     "iterations": runs[-1]["iterations"]},
+        "cpu_baseline": {"value": round(value, 4), "unit": "s", "cores": 1, "kind": "reference",
+                         "sample": "the reference's own CUDA programs (compiled unmodified for sm_100a) "
+                                   "on the full workload, one host thread driving the GPU, wall clock "
+                                   "of build_model + int32 convert + spvi_2"},
+        "e2e": {"value": round(value, 4), "unit": "s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+        "clocks": clocks,
+    }
+
+
+def profile_case():
+    """Small case of the same kernels for ncu: the workload's grid, headings,
+    realisations and modes with nt=30 (fields 0.1 GB, model 0.4 GB > L2); one
+    build and one Jacobi solve (30 sweeps of the fused VI kernel)."""
+    import dataclasses
+
+    import torch
+
+    from e2e_gpu_dp_b200 import api
+    from e2e_gpu_dp_b200.problem import config, make_fields
+
+    prob, spec = config(WORKLOAD, seed=1234)
+    prob = dataclasses.replace(prob, nt=30)
+    fields = make_fields(prob, spec)
+    dev = {k: torch.from_numpy(np.ascontiguousarray(v)).cuda() for k, v in fields.items()}
+    m = api.build_model(prob, dev)
+    _, _, st = m.solve(method="jacobi", threshold=0.1)
+    inf = m.info()
+    print(json.dumps({"profile_case": "c2 geometry, nt=30", "nnz": inf["nnz"], "rows": inf["n_rows"],
+                      "build_kernel_ms": inf["build_kernel_ms"], "jacobi_sweeps": st["iterations"],
+                      "bytes_per_sweep": st["bytes_per_sweep"], "jacobi_s": st["seconds"]}))
+    m.free()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--profile-case", action="store_true", help="small case for ncu captures")
+    args = ap.parse_args()
+    if args.profile_case:
+        return profile_case()
+    ws, rank, local = _dist()
+    if args.impl == "reference":
+        out = run_reference(args, ws, rank, local)
+        if out is not None:
+            print(json.dumps(out), flush=True)
+        return 0
+    if ws > 1:
+        import torch
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=600))
+    try:
+        line = run_ours(args, ws, rank, local)
+        if rank == 0:
+            print(json.dumps(line), flush=True)
+    finally:
+        if ws > 1:
+            import torch.distributed as dist
+
+            dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

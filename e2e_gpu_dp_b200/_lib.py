@@ -56,7 +56,8 @@ class ModelInfo(C.Structure):
         ("nt", C.c_int32), ("ncells", C.c_int32), ("nrzns", C.c_int32), ("count_type", C.c_int32),
         ("index_bits", C.c_int32), ("row_ptr", C.c_void_p), ("col", C.c_void_p),
         ("cnt", C.c_void_p), ("R", C.c_void_p), ("dropped", C.c_uint64),
-        ("overflow_units", C.c_uint64),
+        ("overflow_units", C.c_uint64), ("build_kernel_ms", C.c_double),
+        ("assemble_ms", C.c_double), ("build_launches", C.c_int32), ("reserved", C.c_int32),
     ]
 
 

@@ -107,9 +107,10 @@ class Model:
         o = _lib.ViOpts(1 if method == "layered" else 0, threshold, max_iter, timeout_s,
                         1 if fp64_check else 0, 0)
         stats = _lib.ViStats()
-        if value is not None and _is_device(value):
+        if value is not None and hasattr(value, "data_ptr"):
+            where = _lib.E2E_DEVICE if _is_device(value) else _lib.E2E_HOST
             st = lib().e2e_spvi_solve(self.handle, C.byref(o), policy.data_ptr(), value.data_ptr(),
-                                      _lib.E2E_DEVICE, C.byref(stats), _stream_ptr(stream))
+                                      where, C.byref(stats), _stream_ptr(stream))
             V, pi = value, policy
         else:
             V = np.zeros(ns, np.float32)

@@ -430,6 +430,12 @@ e2e_status run_build(const e2e_problem* p, const DevFields& F, const BuildPlan& 
   uint32_t* pool = nullptr;
   unsigned long long hc[CTR_COUNT];
   const int mm = p->neighb_gsize * p->neighb_gsize;
+  cudaEvent_t ev[4];
+  for (int k = 0; k < 4; ++k) CK(cudaEventCreate(&ev[k]));
+  struct EvFree {
+    cudaEvent_t* e;
+    ~EvFree() { for (int k = 0; k < 4; ++k) cudaEventDestroy(e[k]); }
+  } evfree{ev};
   for (int attempt = 0; attempt < 3; ++attempt) {
     if (!stage_col) {
       CK(cudaMallocAsync((void**)&stage_col, sizeof(int32_t) * (size_t)cap, st));
@@ -453,7 +459,10 @@ e2e_status run_build(const e2e_problem* p, const DevFields& F, const BuildPlan& 
     A.R = m->R;
     A.pool = pool;
     A.pool_units = pool_units;
+    CK(cudaEventRecord(ev[0], st));
     CK(launch_build_tiles(A, pl.count_bits, p->nt - 1, st));
+    CK(cudaEventRecord(ev[1], st));
+    m->build_launches++;
     CK(cudaMemcpyAsync(hc, ctr, sizeof(hc), cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
     bool again = false;
@@ -506,6 +515,7 @@ e2e_status run_build(const e2e_problem* p, const DevFields& F, const BuildPlan& 
   scratch->add(canon);
   CK(cudaMallocAsync((void**)&total, sizeof(int64_t), st));
   scratch->add(total);
+  CK(cudaEventRecord(ev[2], st));
   CK(launch_scan_tiles(tile_len, pl.n_tiles, canon, total, st));
   AssembleArgs S;
   S.n_tiles = pl.n_tiles;
@@ -524,10 +534,13 @@ e2e_status run_build(const e2e_problem* p, const DevFields& F, const BuildPlan& 
   S.col = m->col;
   S.cnt = m->cnt;
   CK(launch_assemble(S, pl.count_bits, m->index_bits, st));
-  if (pl.n_tiles == 0) {
-    // no rows at all (cannot happen for nt >= 2, kept for completeness)
-    CK(cudaMemsetAsync(m->row_ptr, 0, (size_t)pb, st));
-  }
+  CK(cudaEventRecord(ev[3], st));
+  CK(cudaEventSynchronize(ev[3]));
+  float ms = 0.f;
+  CK(cudaEventElapsedTime(&ms, ev[0], ev[1]));
+  m->build_kernel_ms = ms;
+  CK(cudaEventElapsedTime(&ms, ev[2], ev[3]));
+  m->assemble_ms = ms;
   return E2E_OK;
 }
 
@@ -558,6 +571,9 @@ extern "C" e2e_status e2e_model_get_info(const e2e_model* m, e2e_model_info* inf
   info->R = m->R;
   info->dropped = m->dropped;
   info->overflow_units = m->overflow_rows;
+  info->build_kernel_ms = m->build_kernel_ms;
+  info->assemble_ms = m->assemble_ms;
+  info->build_launches = m->build_launches;
   return E2E_OK;
 }
 

@@ -23,6 +23,8 @@ struct e2e_model {
   void* cnt = nullptr;       // device
   float* R = nullptr;        // device, ns * na (state-major)
   uint64_t dropped = 0, misbinned = 0, overflow_rows = 0;
+  double build_kernel_ms = 0, assemble_ms = 0;
+  int32_t build_launches = 0;
   bool layered = false;      // every transition of a layer-t state leads into layer t+1
   e2e_problem prob{};
   bool has_prob = false;

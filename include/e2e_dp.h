@@ -124,6 +124,10 @@ typedef struct {
   const float* R;        /* device, ns * num_actions, state-major */
   uint64_t dropped;      /* samples outside the m x m neighbourhood (not counted, as the reference's bin m*m) */
   uint64_t overflow_units; /* rows whose samples spread beyond the builder's fast window */
+  double build_kernel_ms;  /* device time of the last builder launch (CUDA events on the build stream) */
+  double assemble_ms;      /* device time of the CSR assembly (tile scan + copy) */
+  int32_t build_launches;  /* builder launches (1, or 2 after a re-run with larger buffers) */
+  int32_t reserved;
 } e2e_model_info;
 
 typedef struct e2e_model e2e_model;
