@@ -90,6 +90,8 @@ SIGNATURES = {
     "e2e_model_read_npy": (C.c_int, [C.c_char_p, C.POINTER(C.c_void_p), C.c_void_p]),
     "e2e_spvi_solve": (C.c_int, [C.c_void_p, C.POINTER(ViOpts), C.c_void_p, C.c_void_p, C.c_int,
                                  C.POINTER(ViStats), C.c_void_p]),
+    "e2e_spvi_solve_noalloc": (C.c_int, [C.c_void_p, C.POINTER(ViOpts), C.c_void_p, C.c_void_p,
+                                         C.POINTER(ViStats), C.c_void_p]),
 }
 
 _lib = None

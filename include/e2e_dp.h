@@ -202,6 +202,20 @@ e2e_status e2e_spvi_solve(const e2e_model* m, const e2e_vi_opts* opts /* may be 
                           int32_t* policy_out, float* value_out, int out_where,
                           e2e_vi_stats* stats /* may be NULL */, void* stream);
 
+/* ---- solve without device allocation ----------------------------------------
+ * No counterpart in the reference.  For callers that cannot allocate device
+ * memory (a serving loop whose memory is fully reserved by its own pool, or code
+ * running while another framework's allocator owns the device).  Same sweeps
+ * and results as e2e_spvi_solve, outputs in caller-provided DEVICE buffers; its
+ * scratch is a fixed 32 MiB file-scope device array, so models above
+ * 8,372,224 states (or solves above 8190 sweeps, or fp64_check) are rejected
+ * with E2E_ERR_UNSUPPORTED.  The first call on a device caches the array's
+ * address (make it before any stream capture); all calls share the array, so
+ * calls that overlap on the GPU race. */
+e2e_status e2e_spvi_solve_noalloc(const e2e_model* m, const e2e_vi_opts* opts /* may be NULL */,
+                                  int32_t* policy_dev, float* value_dev,
+                                  e2e_vi_stats* stats /* may be NULL */, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
