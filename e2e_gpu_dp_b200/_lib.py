@@ -77,6 +77,7 @@ SIGNATURES = {
     "e2e_abi_version": (C.c_int, []),
     "e2e_status_string": (C.c_char_p, [C.c_int]),
     "e2e_last_error": (C.c_char_p, []),
+    "e2e_memory_trim": (C.c_int, []),
     "e2e_problem_from_params": (C.c_int, [C.POINTER(C.c_float), C.POINTER(Problem)]),
     "e2e_problem_to_params": (C.c_int, [C.POINTER(Problem), C.POINTER(C.c_float)]),
     "e2e_action_table": (C.c_int, [C.POINTER(Problem)] + [C.POINTER(C.c_float)] * 4),

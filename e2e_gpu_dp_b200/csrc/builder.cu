@@ -28,34 +28,84 @@
 
 namespace e2e {
 
-static constexpr int kWin = 7;            // fast window side
-static constexpr int kWinWords = 25;      // ceil(49 / 2) packed 16-bit counters
+static constexpr int kWin = 8;        // fast window side: bin = li * 8 + lj
+static constexpr int kWinBins = kWin * kWin;
+static constexpr int kNb = 6;         // per-cell obstacle bitmap radius (13 x 13 around S1)
+static constexpr int kNbSide = 2 * kNb + 1;
+static constexpr int kNbBits = kNbSide * kNbSide;
+static constexpr int kNbWords = (kNbBits + 31) / 32;
 
 enum : int { MODE_WINDOW = 0, MODE_FIXED = 1, MODE_DENSE = 2, MODE_LOST = 3 };
+enum : int { MASK_OVR = 0, MASK_INWIN = 1, MASK_EDGE = 2, MASK_TERM = 3, MASK_SLOW = 4, MASK_COUNT = 5 };
 
-template <typename CntT>
+__device__ __forceinline__ bool bit64(uint64_t m, int b) { return (m >> b) & 1ull; }
+
+static constexpr int kRcw = 64;                 // realisations per warp-private velocity chunk
+static constexpr int kVelStride = kRcw + 1;     // padded: the cells of a warp hit distinct banks
+static constexpr uint32_t kOvrFlag = 0x8000u;   // counter bit 15: bin is obstacle-overridden
+static constexpr uint32_t kCountMask = 0x7FFFu;
+
+// Column of a thread in the 16-bit counter rows: lane l of warps 2p and 2p+1
+// share the 32-bit word 32p + l, so a warp's 32 lanes hit 32 distinct banks
+// whatever bins they update.
+__device__ __forceinline__ int counter_col(int warp, int lane) {
+  return 64 * (warp >> 1) + 2 * lane + (warp & 1);
+}
+__host__ __device__ __forceinline__ int counter_log2_stride(int nthr) {
+  int l = 6;
+  while ((1 << l) < nthr) ++l;
+  return l;
+}
+
+// K1.  Template: CntT = staged count type; UNIT = unit cell spacing.
+//
+// A CTA owns 32 consecutive cells of one layer and all their actions.  Warp w
+// holds cells_per_warp = 32/P cells (P = next power of two >= Na) and lane
+// (c, a) is the row (cell c, action a), so a warp computes the velocities of
+// its own cells (u + sum_k ui_k*Y_k, reference order) into warp-private
+// shared memory, samples without CTA barriers and emits its own rows.
+//
+// Per row the 8x8 window of the grid around the mean-flow landing cell is
+// classified once.  The obstacle override is bit 15 of the bin's 16-bit
+// counter; masks kept in shared memory mark `edge` (boundary ring), `term`
+// (terminal subgrid) and `slow` bins (outside the m x m neighbourhood, or a
+// reward that reads the scalar field).  The reward of a landing is a table
+// entry: k = number of r_outbound additions (x clamp, y clamp, edge), terminal
+// or not, indexing tab[a] = the reference's float operations evaluated once
+// per action (exact for every float input).  Warps without edge/terminal/slow
+// bins run a loop that needs none of the masks.  A sample that leaves the
+// window (or lands on a slow bin) is only counted; a rescan of the chunk runs
+// the full reference expression for it afterwards, so its reward joins the
+// row's sum after the chunk's in-window rewards.
+template <typename CntT, bool UNIT>
 __global__ void __launch_bounds__(1024) k_build_tiles(BuildArgs A) {
   extern __shared__ __align__(16) unsigned char smem[];
   const DevProblem& P = A.P;
   const int nthr = blockDim.x;
   const int tid = threadIdx.x;
   const int lane = tid & 31;
-  const int a = tid >> 5;
+  const int warp = tid >> 5;
   const int nwarps = nthr >> 5;
+  const int lanes_log2 = A.lanes_log2;           // P = 1 << lanes_log2 >= na
+  const int a = lane & ((1 << lanes_log2) - 1);  // action of this lane
+  const int cw = lane >> lanes_log2;             // cell within warp
+  const int cl = warp * (32 >> lanes_log2) + cw; // cell within tile (0..31)
   const int T = A.t0 + blockIdx.y;
   const int g = P.g;
   const int64_t nc = (int64_t)g * g;
   const int64_t c0 = (int64_t)blockIdx.x * 32;
-  const int64_t cell = c0 + lane;
-  const bool valid = cell < nc;
+  const int64_t cell = c0 + cl;
+  const bool valid = (cell < nc) && (a < P.na);
   const int nm = P.nm;
+  const int log2S = counter_log2_stride(nthr);
 
-  float2* vel = reinterpret_cast<float2*>(smem);                     // rc x 32
-  float* modes = reinterpret_cast<float*>(vel + (size_t)A.rc * 32);  // 2*nm x 32
-  uint32_t* win = reinterpret_cast<uint32_t*>(modes + 2 * nm * 32);  // kWinWords x nthr
-  int* scan = reinterpret_cast<int*>(win + kWinWords * nthr);        // nthr
-  __shared__ int warp_tot[32];
-  __shared__ unsigned long long tile_base_sh;
+  float* modes = reinterpret_cast<float*>(smem);                           // 2*nm x 32
+  float2* velw = reinterpret_cast<float2*>(modes + 2 * nm * 32);           // 32 x kVelStride
+  uint64_t* masks = reinterpret_cast<uint64_t*>(velw + 32 * kVelStride);   // MASK_COUNT x nthr
+  uint16_t* win = reinterpret_cast<uint16_t*>(masks + MASK_COUNT * nthr);  // 64 x S
+  __shared__ uint32_t obsmap[32][kNbWords];
+  __shared__ float tab[32][8];
+  uint16_t* const wcol = win + counter_col(warp, lane);
 
   // ---- stage the modes of the tile's cells (ui then vi) -------------------
   for (int idx = tid; idx < 2 * nm * 32; idx += nthr) {
@@ -68,20 +118,53 @@ __global__ void __launch_bounds__(1024) k_build_tiles(BuildArgs A) {
     }
     modes[idx] = val;
   }
+  for (int idx = tid; idx < 32 * kNbWords; idx += nthr) obsmap[idx / kNbWords][idx % kNbWords] = 0u;
+  const bool late = T > P.nt - 20;
+  const bool rad = (P.reward_type == 2 || P.reward_type == 3);
+  if (tid < P.na) {
+    // landing rewards after k r_outbound additions, then terminal or late, then
+    // the step reward: move() + transition_calc's `r += r_step` (:343-354, :533)
+    const float Fa = P.ac_speed[tid];
+    const float r_step = step_reward(P, Fa, 0.f, 0.f);
+    float tk = 0;
+    for (int k = 0; k < 4; ++k) {
+      float r = tk;
+      if (late) r += 0.05 * P.r_out;
+      r += r_step;
+      tab[tid][k] = r;
+      float rt = tk;
+      rt += P.r_term;
+      rt += r_step;
+      tab[tid][4 + k] = rt;
+      tk += P.r_out;
+    }
+  }
+  __syncthreads();
+  // ---- obstacle override of S1 -> S2 for S2 within 6 cells of S1, per cell
+  // (goes_through_obstacle, src/build_model.cu:444-477), shared by the actions
+  for (int idx = tid; idx < 32 * kNbBits; idx += nthr) {
+    const int c = idx / kNbBits, b = idx - c * kNbBits;
+    const int64_t cc = c0 + c;
+    if (cc >= nc) continue;
+    const int ci1 = (int)(cc / g), cj1 = (int)(cc - (int64_t)ci1 * g);
+    const int i2 = ci1 + b / kNbSide - kNb, j2 = cj1 + b % kNbSide - kNb;
+    if (i2 < 0 || i2 >= g || j2 < 0 || j2 >= g) continue;
+    if (through_obstacle(P, A.F.mask, T, ci1, cj1, i2, j2)) atomicOr(&obsmap[c][b >> 5], 1u << (b & 31));
+  }
 
   // ---- per-row set-up -------------------------------------------------------
   const int i1 = valid ? (int)(cell / g) : 0;
   const int j1 = valid ? (int)(cell - (int64_t)i1 * g) : 0;
   const float x1 = P.xs[j1];
   const float y1 = P.ys[g - 1 - i1];
-  const float F = P.ac_speed[a];
-  const float cs = P.ac_cos[a];
-  const float sn = P.ac_sin[a];
-  const bool late = T > P.nt - 20;
-  const bool rad = (P.reward_type == 2 || P.reward_type == 3);
-  const float u1 = valid ? __ldg(A.F.u + (int64_t)T * nc + cell) : 0.f;
-  const float v1 = valid ? __ldg(A.F.v + (int64_t)T * nc + cell) : 0.f;
-  const float rad1 = (valid && rad) ? __ldg(A.F.s + (int64_t)T * nc + cell) : 0.f;
+  const int aa = a < P.na ? a : 0;
+  const float F = P.ac_speed[aa];
+  const float cs = P.ac_cos[aa];
+  const float sn = P.ac_sin[aa];
+  const bool cvalid = cell < nc;
+  const float u1 = cvalid ? __ldg(A.F.u + (int64_t)T * nc + cell) : 0.f;
+  const float v1 = cvalid ? __ldg(A.F.v + (int64_t)T * nc + cell) : 0.f;
+  const float rad1 = (cvalid && rad) ? __ldg(A.F.s + (int64_t)T * nc + cell) : 0.f;
   const int W = g < kWin ? g : kWin;
 
   int mode = MODE_WINDOW;
@@ -94,101 +177,216 @@ __global__ void __launch_bounds__(1024) k_build_tiles(BuildArgs A) {
     mode = MODE_FIXED;  // obstacle S1: no move, r = r_outbound (:542-544)
     r_fixed = P.r_out;
   }
+  __syncthreads();  // obsmap complete
+  for (int b = 0; b < kWinBins; ++b) wcol[b << log2S] = 0;
   int wi0 = 0, wj0 = 0;
-  uint64_t ovr = 0, inwin = 0;
+  uint64_t ovr = 0, inwin = 0, edge = 0, term = 0, slow = 0;
   if (mode == MODE_WINDOW) {
     int ci, cj;
-    float rdummy;
-    move_sample(P, F, cs, sn, u1, v1, x1, y1, late, ci, cj, rdummy);
-    wi0 = min(max(ci - kWin / 2, 0), g - W);
-    wj0 = min(max(cj - kWin / 2, 0), g - W);
+    land<UNIT>(P, F, cs, sn, u1, v1, x1, y1, ci, cj);
+    // window around the mean landing, inside the m x m neighbourhood when the
+    // grid allows it, always inside the grid
+    wi0 = min(max(ci - (kWin / 2 - 1), i1 - P.del), i1 + P.del - W + 1);
+    wj0 = min(max(cj - (kWin / 2 - 1), j1 - P.del), j1 + P.del - W + 1);
+    wi0 = min(max(wi0, 0), g - W);
+    wj0 = min(max(wj0, 0), g - W);
     for (int li = 0; li < W; ++li) {
       for (int lj = 0; lj < W; ++lj) {
-        int i2 = wi0 + li, j2 = wj0 + lj;
-        int lb = li * kWin + lj;
-        int di = i2 - i1 + P.del, dj = j2 - j1 + P.del;
-        if (di >= 0 && di < P.m && dj >= 0 && dj < P.m) inwin |= 1ull << lb;
-        if (through_obstacle(P, A.F.mask, T, i1, j1, i2, j2)) ovr |= 1ull << lb;
+        const int i2 = wi0 + li, j2 = wj0 + lj;
+        const int b = li * kWin + lj;
+        const int di = i2 - i1, dj = j2 - j1;
+        const bool inw = di >= -P.del && di <= P.del && dj >= -P.del && dj <= P.del;
+        bool o;
+        if (di >= -kNb && di <= kNb && dj >= -kNb && dj <= kNb) {
+          const int nb = (di + kNb) * kNbSide + (dj + kNb);
+          o = (obsmap[cl][nb >> 5] >> (nb & 31)) & 1u;
+        } else {
+          o = through_obstacle(P, A.F.mask, T, i1, j1, i2, j2);
+        }
+        if (inw) inwin |= 1ull << b;
+        if (o) {
+          ovr |= 1ull << b;
+          wcol[b << log2S] = (uint16_t)kOvrFlag;
+        }
+        if (i2 == 0 || i2 == g - 1 || j2 == 0 || j2 == g - 1) edge |= 1ull << b;
+        if (is_terminal(P, i2, j2)) term |= 1ull << b;
+        if (!inw || rad) slow |= 1ull << b;
       }
     }
   }
-#pragma unroll
-  for (int w = 0; w < kWinWords; ++w) win[w * nthr + tid] = 0u;
+  masks[MASK_OVR * nthr + tid] = ovr;
+  masks[MASK_INWIN * nthr + tid] = inwin;
+  masks[MASK_EDGE * nthr + tid] = edge;
+  masks[MASK_TERM * nthr + tid] = term;
+  masks[MASK_SLOW * nthr + tid] = slow;
+  // a warp takes the general loop if any of its rows can land on an edge,
+  // terminal or slow bin
+  const bool plain_row = (mode != MODE_WINDOW) || ((edge | term | slow) == 0);
+  const bool plain_warp = __all_sync(0xffffffffu, plain_row);
+  const float r_plain = tab[aa][0];
 
   float sumR = 0.f;
   uint32_t n_drop = 0, n_misbin = 0;
   uint32_t* dense = nullptr;
   const int mm = P.m * P.m;
+  float2* myvel = velw + cl * kVelStride;   // this lane's cell
+  const int per = 1 << lanes_log2;         // lanes sharing a cell
+  // constants of the sample loops, held in registers
+  const float xs0 = P.xs0, ysn = P.ysn, axmax = P.axmax, aymax = P.aymax;
+  const float xsn = P.xsn, ys0 = P.ys0, dt = P.dt, r_out = P.r_out;
+  const int kx = 0x4B400000 + wj0;  // float bits of 1.5*2^23 plus the window origin:
+  const int ky = 0x4B400000 + wi0;  // round_half_up_index then gives window-local indices
 
-  // ---- realisations in chunks ---------------------------------------------
-  for (int base = 0; base < P.nrzns; base += A.rc) {
-    const int clen = min(A.rc, P.nrzns - base);
-    __syncthreads();  // modes staged / previous chunk consumed
-    for (int q = a; q < clen; q += nwarps) {
-      const float* y = A.F.Y + ((int64_t)T * P.nrzns + base + q) * nm;
-      float sum_x = 0;
-      float sum_y = 0;
-      for (int k = 0; k < nm; k++) sum_x += modes[k * 32 + lane] * __ldg(y + k);
-      for (int k = 0; k < nm; k++) sum_y += modes[(nm + k) * 32 + lane] * __ldg(y + k);
-      // extract_velocity, src/build_model.cu:389-401: mean + sum over modes
-      vel[q * 32 + lane] = make_float2(u1 + sum_x, v1 + sum_y);
+  // Full reference expression for one sample (rare): reward, counts, dense
+  // switch and drop accounting.
+  auto full_sample = [&](float vx, float vy, int i2, int j2) -> float {
+    int k2, l2;
+    float r;
+    move_sample<UNIT>(P, F, cs, sn, vx, vy, x1, y1, late, k2, l2, r);
+    float rad2 = 0.f;
+    if (rad) rad2 = __ldg(A.F.s + (int64_t)(T + 1) * nc + (int64_t)i2 * g + j2);
+    float r_step = step_reward(P, F, rad1, rad2);
+    r += r_step;
+    const unsigned li = (unsigned)(i2 - wi0), lj = (unsigned)(j2 - wj0);
+    if (mode == MODE_WINDOW && li < (unsigned)W && lj < (unsigned)W) {
+      const int b = (int)li * kWin + (int)lj;
+      if (bit64(masks[MASK_OVR * nthr + tid], b)) r = r_out;
+      if (bit64(masks[MASK_INWIN * nthr + tid], b)) {
+        wcol[b << log2S] += 1;
+      } else {
+        n_drop++;
+        if (i2 - i1 + P.del < P.m && j2 - j1 + P.del < P.m) n_misbin++;
+      }
+      return r;
     }
-    __syncthreads();
+    if (through_obstacle(P, A.F.mask, T, i1, j1, i2, j2)) r = r_out;
+    const int di = i2 - i1 + P.del, dj = j2 - j1 + P.del;
+    if (di >= 0 && di < P.m && dj >= 0 && dj < P.m) {
+      if (mode == MODE_WINDOW) {
+        // switch this row to a dense m*m histogram from the pool
+        unsigned long long slot = atomicAdd(A.counters + CTR_POOL, 1ull);
+        atomicAdd(A.counters + CTR_OVERFLOW_ROWS, 1ull);
+        if (slot < (unsigned long long)A.pool_units) {
+          dense = A.pool + slot * (unsigned long long)mm;
+          for (int b = 0; b < mm; ++b) dense[b] = 0u;
+          for (int wl = 0; wl < kWinBins; ++wl) {
+            const uint32_t c = wcol[wl << log2S] & kCountMask;
+            if (c) {
+              const int ii = wi0 + wl / kWin - i1 + P.del, jj = wj0 + wl % kWin - j1 + P.del;
+              dense[ii * P.m + jj] += c;
+            }
+          }
+          mode = MODE_DENSE;
+        } else {
+          mode = MODE_LOST;
+        }
+      }
+      if (mode == MODE_DENSE) dense[di * P.m + dj] += 1u;
+    } else {
+      n_drop++;
+      if (di < P.m && dj < P.m) n_misbin++;
+    }
+    return r;
+  };
+
+  // ---- realisations in warp-private chunks ----------------------------------
+  for (int base = 0; base < P.nrzns; base += kRcw) {
+    const int clen = min(kRcw, P.nrzns - base);
+    __syncwarp();  // previous chunk consumed
+    for (int q = a; q < clen; q += per) {
+      if (cvalid) {
+        const float* y = A.F.Y + ((int64_t)T * P.nrzns + base + q) * nm;
+        float sum_x = 0;
+        float sum_y = 0;
+        for (int k = 0; k < nm; k++) sum_x += modes[k * 32 + cl] * __ldg(y + k);
+        for (int k = 0; k < nm; k++) sum_y += modes[(nm + k) * 32 + cl] * __ldg(y + k);
+        // extract_velocity, src/build_model.cu:389-401: mean + sum over modes
+        myvel[q] = make_float2(u1 + sum_x, v1 + sum_y);
+      }
+    }
+    __syncwarp();
     if (mode == MODE_FIXED) {
       for (int q = 0; q < clen; ++q) sumR += r_fixed;
-    } else if (mode != MODE_LOST) {
-      for (int q = 0; q < clen; ++q) {
-        const float2 vv = vel[q * 32 + lane];
-        int i2, j2;
-        float r;
-        move_sample(P, F, cs, sn, vv.x, vv.y, x1, y1, late, i2, j2, r);
-        float rad2 = 0.f;
-        if (rad) rad2 = __ldg(A.F.s + (int64_t)(T + 1) * nc + (int64_t)i2 * g + j2);
-        float r_step = step_reward(P, F, rad1, rad2);
-        r += r_step;
-        const unsigned li = (unsigned)(i2 - wi0), lj = (unsigned)(j2 - wj0);
-        if (mode == MODE_WINDOW && li < (unsigned)W && lj < (unsigned)W) {
-          const int lb = (int)li * kWin + (int)lj;
-          if ((ovr >> lb) & 1ull) r = P.r_out;
-          if ((inwin >> lb) & 1ull) {
-            win[(lb >> 1) * nthr + tid] += 1u << ((lb & 1) << 4);
-          } else {
-            n_drop++;
-            int di = i2 - i1 + P.del, dj = j2 - j1 + P.del;
-            if (di < P.m && dj < P.m) n_misbin++;
-          }
-        } else {
-          if (through_obstacle(P, A.F.mask, T, i1, j1, i2, j2)) r = P.r_out;
-          const int di = i2 - i1 + P.del, dj = j2 - j1 + P.del;
-          if (di >= 0 && di < P.m && dj >= 0 && dj < P.m) {
-            if (mode == MODE_WINDOW) {
-              // switch this row to a dense m*m histogram from the pool
-              unsigned long long slot = atomicAdd(A.counters + CTR_POOL, 1ull);
-              atomicAdd(A.counters + CTR_OVERFLOW_ROWS, 1ull);
-              if (slot < (unsigned long long)A.pool_units) {
-                dense = A.pool + slot * (unsigned long long)mm;
-                for (int b = 0; b < mm; ++b) dense[b] = 0u;
-                for (int lb = 0; lb < W * kWin; ++lb) {
-                  if ((lb % kWin) >= W) continue;
-                  uint32_t c = (win[(lb >> 1) * nthr + tid] >> ((lb & 1) << 4)) & 0xFFFFu;
-                  if (c) {
-                    int ii = wi0 + lb / kWin - i1 + P.del, jj = wj0 + lb % kWin - j1 + P.del;
-                    dense[ii * P.m + jj] += c;
-                  }
-                }
-                mode = MODE_DENSE;
-              } else {
-                mode = MODE_LOST;
-              }
-            }
-            if (mode == MODE_DENSE) dense[di * P.m + dj] += 1u;
-          } else {
-            n_drop++;
-            if (di < P.m && dj < P.m) n_misbin++;
-          }
+    } else if (mode == MODE_WINDOW) {
+      int n_out = 0;
+      if (plain_warp) {
+#pragma unroll 4
+        for (int q = 0; q < clen; ++q) {
+          const float2 vv = myvel[q];
+          float vnetx = F * cs + vv.x;  // move(), src/build_model.cu:284-289
+          float vnety = F * sn + vv.y;
+          float xnew = x1 + (vnetx * dt);
+          float ynew = y1 + (vnety * dt);
+          const float ax = fminf(fmaxf(xnew - xs0, 0.0f), axmax);
+          const float ay = fminf(fmaxf(-(ynew - ysn), 0.0f), aymax);
+          const int lj = round_half_up_index(ax, kx);
+          const int li = round_half_up_index(ay, ky);
+          const bool inw = (unsigned)(li | lj) < (unsigned)kWin;
+          const int b = inw ? (li << 3) + lj : 0;
+          uint16_t* wp = wcol + (b << log2S);
+          const uint32_t w = *wp;
+          const float r = (w & kOvrFlag) ? r_out : r_plain;
+          *wp = (uint16_t)(inw ? w + 1 : w);  // branch-free: a miss writes bin 0 back
+          const float s2 = sumR + r;
+          sumR = inw ? s2 : sumR;
+          n_out += inw ? 0 : 1;
         }
-        sumR += r;
-        if (mode == MODE_LOST) break;
+      } else {
+        const uint64_t m_edge = masks[MASK_EDGE * nthr + tid];
+        const uint64_t m_term = masks[MASK_TERM * nthr + tid];
+        const uint64_t m_slow = masks[MASK_SLOW * nthr + tid];
+        for (int q = 0; q < clen; ++q) {
+          const float2 vv = myvel[q];
+          float vnetx = F * cs + vv.x;
+          float vnety = F * sn + vv.y;
+          float xnew = x1 + (vnetx * dt);
+          float ynew = y1 + (vnety * dt);
+          const int kcl = ((xnew > xsn) || (xnew < xs0) ? 1 : 0) + ((ynew > ysn) || (ynew < ys0) ? 1 : 0);
+          int li, lj;
+          if (UNIT) {
+            const float ax = fminf(fmaxf(xnew - xs0, 0.0f), axmax);
+            const float ay = fminf(fmaxf(-(ynew - ysn), 0.0f), aymax);
+            lj = round_half_up_index(ax, kx);
+            li = round_half_up_index(ay, ky);
+          } else {
+            int i2, j2;
+            land<UNIT>(P, F, cs, sn, vv.x, vv.y, x1, y1, i2, j2);
+            li = i2 - wi0;
+            lj = j2 - wj0;
+          }
+          const bool inw = (unsigned)(li | lj) < (unsigned)kWin;
+          const int b = inw ? (li << 3) + lj : 0;
+          const bool fast = inw && !bit64(m_slow, b);
+          uint16_t* wp = wcol + (b << log2S);
+          const uint32_t w = *wp;
+          const int k = kcl + (bit64(m_edge, b) ? 1 : 0);
+          float r = tab[aa][(bit64(m_term, b) ? 4 : 0) + k];
+          if (w & kOvrFlag) r = r_out;
+          *wp = (uint16_t)(fast ? w + 1 : w);
+          const float s2 = sumR + r;
+          sumR = fast ? s2 : sumR;
+          n_out += fast ? 0 : 1;
+        }
+      }
+      if (n_out) {
+        // rescan: the chunk's samples that left the window or hit a slow bin
+        const uint64_t m_slow = masks[MASK_SLOW * nthr + tid];
+        for (int q = 0; q < clen; ++q) {
+          const float2 vv = myvel[q];
+          int i2, j2;
+          land<UNIT>(P, F, cs, sn, vv.x, vv.y, x1, y1, i2, j2);
+          const int li = i2 - wi0, lj = j2 - wj0;
+          const bool inw = (unsigned)(li | lj) < (unsigned)kWin;
+          if (inw && !bit64(m_slow, (li << 3) + lj)) continue;
+          sumR += full_sample(vv.x, vv.y, i2, j2);
+        }
+      }
+    } else if (mode == MODE_DENSE) {
+      for (int q = 0; q < clen; ++q) {
+        const float2 vv = myvel[q];
+        int i2, j2;
+        land<UNIT>(P, F, cs, sn, vv.x, vv.y, x1, y1, i2, j2);
+        sumR += full_sample(vv.x, vv.y, i2, j2);
       }
     }
   }
@@ -196,63 +394,40 @@ __global__ void __launch_bounds__(1024) k_build_tiles(BuildArgs A) {
   if (n_misbin) atomicAdd(A.counters + CTR_MISBIN, (unsigned long long)n_misbin);
   if (mode == MODE_LOST) atomicOr(reinterpret_cast<unsigned int*>(A.counters + CTR_FLAGS), FLAG_POOL_EXHAUSTED);
 
-  // ---- row lengths, tile scan, emission ------------------------------------
+  // ---- per-warp emission: row lengths, warp scan, one atomicAdd -----------
   int nnz = 0;
   if (valid) {
     if (mode == MODE_FIXED) {
       nnz = 1;
     } else if (mode == MODE_WINDOW) {
-#pragma unroll
-      for (int w = 0; w < kWinWords; ++w) {
-        uint32_t word = win[w * nthr + tid];
-        nnz += ((word & 0xFFFFu) != 0u) + ((word >> 16) != 0u);
-      }
+      for (int wl = 0; wl < kWinBins; ++wl) nnz += (wcol[wl << log2S] & kCountMask) != 0;
     } else if (mode == MODE_DENSE) {
       for (int b = 0; b < mm; ++b) nnz += dense[b] != 0u;
     }
   }
-  const int lrow = lane * P.na + a;  // row order inside the tile: cell-major, then action
-  __syncthreads();
-  scan[lrow] = nnz;
-  __syncthreads();
-  // exclusive scan over scan[0..nthr) in place
-  int v = scan[tid];
-  int incl = v;
+  // lane order = (cell, action) order of the warp's rows; padding lanes add 0
+  int incl = nnz;
 #pragma unroll
   for (int o = 1; o < 32; o <<= 1) {
     int t2 = __shfl_up_sync(0xffffffffu, incl, o);
     if (lane >= o) incl += t2;
   }
-  if (lane == 31) warp_tot[a] = incl;
-  __syncthreads();
-  if (a == 0) {
-    int wt = lane < nwarps ? warp_tot[lane] : 0;
-    int wi = wt;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-      int t2 = __shfl_up_sync(0xffffffffu, wi, o);
-      if (lane >= o) wi += t2;
-    }
-    if (lane < nwarps) warp_tot[lane] = wi - wt;  // exclusive warp offsets
-    if (lane == 31) {
-      // wi on lane 31 is the tile total
-      tile_base_sh = atomicAdd(A.counters + CTR_STAGE, (unsigned long long)wi);
-      const int64_t tile = (int64_t)T * A.tiles_per_layer + blockIdx.x;
-      A.tile_base[tile] = (int64_t)tile_base_sh;
-      A.tile_len[tile] = wi;
-    }
+  const int total = __shfl_sync(0xffffffffu, incl, 31);
+  unsigned long long wbase = 0;
+  if (lane == 0) {
+    wbase = atomicAdd(A.counters + CTR_STAGE, (unsigned long long)total);
+    const int64_t tile = ((int64_t)T * A.tiles_per_layer + blockIdx.x) * nwarps + warp;
+    A.tile_base[tile] = (int64_t)wbase;
+    A.tile_len[tile] = total;
   }
-  __syncthreads();
-  scan[tid] = warp_tot[a] + incl - v;
-  __syncthreads();
+  wbase = __shfl_sync(0xffffffffu, wbase, 0);
   if (!valid) return;
-  const int excl = scan[lrow];
+  const int excl = incl - nnz;
   const int64_t grow = ((int64_t)T * nc + cell) * P.na + a;
   A.row_off[grow] = (uint32_t)excl;
   A.R[grow] = sumR / P.nrzns;  // compute_mean, src/build_model.cu:567
-  const unsigned long long tb = tile_base_sh;
   if (mode == MODE_LOST) return;
-  unsigned long long off = tb + (unsigned long long)excl;
+  unsigned long long off = wbase + (unsigned long long)excl;
   if (off + (unsigned long long)nnz > (unsigned long long)A.stage_cap) return;  // host re-runs
   CntT* scnt = reinterpret_cast<CntT*>(A.stage_cnt);
   const int64_t next_layer = (int64_t)(T + 1) * nc;
@@ -260,10 +435,10 @@ __global__ void __launch_bounds__(1024) k_build_tiles(BuildArgs A) {
     A.stage_col[off] = (int32_t)(next_layer + cell);
     scnt[off] = (CntT)P.nrzns;
   } else if (mode == MODE_WINDOW) {
-    for (int lb = 0; lb < W * kWin; ++lb) {
-      uint32_t c = (win[(lb >> 1) * nthr + tid] >> ((lb & 1) << 4)) & 0xFFFFu;
+    for (int wl = 0; wl < kWinBins; ++wl) {
+      const uint32_t c = wcol[wl << log2S] & kCountMask;
       if (c) {
-        int i2 = wi0 + lb / kWin, j2 = wj0 + lb % kWin;
+        const int i2 = wi0 + wl / kWin, j2 = wj0 + wl % kWin;
         A.stage_col[off] = (int32_t)(next_layer + (int64_t)i2 * g + j2);
         scnt[off] = (CntT)c;
         ++off;
@@ -271,9 +446,9 @@ __global__ void __launch_bounds__(1024) k_build_tiles(BuildArgs A) {
     }
   } else {  // MODE_DENSE: bins in reference order
     for (int b = 0; b < mm; ++b) {
-      uint32_t c = dense[b];
+      const uint32_t c = dense[b];
       if (c) {
-        int i2 = b / P.m + i1 - P.del, j2 = b % P.m + j1 - P.del;
+        const int i2 = b / P.m + i1 - P.del, j2 = b % P.m + j1 - P.del;
         A.stage_col[off] = (int32_t)(next_layer + (int64_t)i2 * g + j2);
         scnt[off] = (CntT)c;
         ++off;
@@ -282,22 +457,36 @@ __global__ void __launch_bounds__(1024) k_build_tiles(BuildArgs A) {
   }
 }
 
-// K2: exclusive scan of the tile lengths (tile order == row order) with one
-// CTA; each thread owns a contiguous run of tiles.
-__global__ void k_scan_tiles(const int32_t* __restrict__ tile_len, int64_t n_tiles,
-                             int64_t* __restrict__ canon, int64_t* __restrict__ total) {
+// K2: exclusive scan of the tile lengths (tile order == row order), in three
+// steps: per-block sums, one block scanning the block sums, per-block scans.
+static constexpr int kScanBlock = 1024;
+
+__global__ void k_scan_sums(const int32_t* __restrict__ len, int64_t n, int64_t* __restrict__ sums) {
+  __shared__ int64_t red[32];
+  const int64_t i = (int64_t)blockIdx.x * kScanBlock + threadIdx.x;
+  int64_t v = i < n ? len[i] : 0;
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    int64_t w = red[threadIdx.x];
+    for (int o = 16; o > 0; o >>= 1) w += __shfl_xor_sync(0xffffffffu, w, o);
+    if (threadIdx.x == 0) sums[blockIdx.x] = w;
+  }
+}
+
+__global__ void k_scan_block_sums(int64_t* sums, int64_t nb, int64_t* total) {
   __shared__ int64_t part[1024];
   const int tid = threadIdx.x;
-  const int nthr = blockDim.x;
-  const int64_t per = (n_tiles + nthr - 1) / nthr;
-  const int64_t b = min((int64_t)tid * per, n_tiles), e = min(b + per, n_tiles);
+  const int64_t per = (nb + 1023) / 1024;
+  const int64_t b = min((int64_t)tid * per, nb), e = min(b + per, nb);
   int64_t s = 0;
-  for (int64_t i = b; i < e; ++i) s += tile_len[i];
+  for (int64_t i = b; i < e; ++i) s += sums[i];
   part[tid] = s;
   __syncthreads();
   if (tid == 0) {
     int64_t run = 0;
-    for (int k = 0; k < nthr; ++k) {
+    for (int k = 0; k < 1024; ++k) {
       int64_t x = part[k];
       part[k] = run;
       run += x;
@@ -307,16 +496,45 @@ __global__ void k_scan_tiles(const int32_t* __restrict__ tile_len, int64_t n_til
   __syncthreads();
   int64_t run = part[tid];
   for (int64_t i = b; i < e; ++i) {
-    canon[i] = run;
-    run += tile_len[i];
+    int64_t x = sums[i];
+    sums[i] = run;
+    run += x;
   }
 }
 
-// K3: one CTA per tile: move the tile's entries from staging to their
-// canonical position and write row_ptr for the tile's rows.
+__global__ void k_scan_finish(const int32_t* __restrict__ len, int64_t n,
+                              const int64_t* __restrict__ sums, int64_t* __restrict__ out) {
+  __shared__ int64_t wsum[32];
+  const int64_t i = (int64_t)blockIdx.x * kScanBlock + threadIdx.x;
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  int64_t v = i < n ? len[i] : 0;
+  int64_t incl = v;
+  for (int o = 1; o < 32; o <<= 1) {
+    int64_t t = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= o) incl += t;
+  }
+  if (lane == 31) wsum[w] = incl;
+  __syncthreads();
+  if (w == 0) {
+    int64_t x = wsum[lane];
+    int64_t xi = x;
+    for (int o = 1; o < 32; o <<= 1) {
+      int64_t t = __shfl_up_sync(0xffffffffu, xi, o);
+      if (lane >= o) xi += t;
+    }
+    wsum[lane] = xi - x;
+  }
+  __syncthreads();
+  if (i < n) out[i] = sums[blockIdx.x] + wsum[w] + incl - v;
+}
+
+// K3: one warp per tile (the rows of one builder warp): move the tile's
+// entries from staging to their canonical position and write row_ptr.
 template <typename CntT, typename PtrT>
 __global__ void k_assemble(AssembleArgs A) {
-  const int64_t tile = blockIdx.x;
+  const int lane = threadIdx.x & 31;
+  const int64_t tile = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  if (tile >= A.n_tiles) return;
   const int64_t src = A.tile_base[tile];
   const int64_t dst = A.canon[tile];
   const int len = A.tile_len[tile];
@@ -324,19 +542,21 @@ __global__ void k_assemble(AssembleArgs A) {
   const CntT* __restrict__ scnt = reinterpret_cast<const CntT*>(A.stage_cnt) + src;
   int32_t* __restrict__ dcol = A.col + dst;
   CntT* __restrict__ dcnt = reinterpret_cast<CntT*>(A.cnt) + dst;
-  for (int k = threadIdx.x; k < len; k += blockDim.x) {
+  for (int k = lane; k < len; k += 32) {
     dcol[k] = scol[k];
     dcnt[k] = scnt[k];
   }
   const int64_t layer = tile / A.tiles_per_layer;
   const int64_t tl = tile - layer * A.tiles_per_layer;
-  const int64_t cb = tl * 32;
-  const int64_t ce = min(cb + 32, A.ncells);
-  const int64_t r0 = (layer * A.ncells + cb) * A.na;
-  const int64_t r1 = (layer * A.ncells + ce) * A.na;
+  const int64_t cb = tl * A.cells_per_tile;
+  const int64_t ce = min(cb + A.cells_per_tile, A.ncells);
   PtrT* rp = reinterpret_cast<PtrT*>(A.row_ptr);
-  for (int64_t r = r0 + threadIdx.x; r < r1; r += blockDim.x) rp[r] = (PtrT)(dst + A.row_off[r]);
-  if (tile == A.n_tiles - 1 && threadIdx.x == 0) rp[A.n_rows] = (PtrT)A.total_nnz;
+  if (cb < ce) {
+    const int64_t r0 = (layer * A.ncells + cb) * A.na;
+    const int64_t r1 = (layer * A.ncells + ce) * A.na;
+    for (int64_t r = r0 + lane; r < r1; r += 32) rp[r] = (PtrT)(dst + A.row_off[r]);
+  }
+  if (tile == A.n_tiles - 1 && lane == 0) rp[A.n_rows] = (PtrT)A.total_nnz;
 }
 
 // Device cosf/sinf of the headings: the values move() multiplies by F
@@ -351,40 +571,53 @@ __global__ void k_action_trig(const float* angle, int n, float* cosv, float* sin
 
 // ---- launch wrappers ---------------------------------------------------------
 
+int build_lanes_log2(int na) {
+  int l = 0;
+  while ((1 << l) < na) ++l;
+  return l;
+}
+
 size_t build_smem_bytes(int na, int nm, int rc) {
-  return (size_t)rc * 32 * sizeof(float2) + (size_t)2 * nm * 32 * sizeof(float) +
-         (size_t)kWinWords * 32 * na * sizeof(uint32_t) + (size_t)32 * na * sizeof(int);
+  (void)rc;
+  const int nthr = 32 << build_lanes_log2(na);
+  return (size_t)2 * nm * 32 * sizeof(float) + (size_t)32 * kVelStride * sizeof(float2) +
+         (size_t)MASK_COUNT * nthr * sizeof(uint64_t) +
+         (size_t)kWinBins * ((size_t)1 << counter_log2_stride(nthr)) * sizeof(uint16_t);
+}
+
+template <typename CntT, bool UNIT>
+static cudaError_t launch_one(const BuildArgs& A, int n_layers, cudaStream_t st) {
+  dim3 grid((unsigned)A.tiles_per_layer, (unsigned)n_layers);
+  dim3 block((unsigned)(32u << A.lanes_log2));
+  size_t sm = build_smem_bytes(A.P.na, A.P.nm, A.rc);
+  cudaError_t e = cudaFuncSetAttribute(k_build_tiles<CntT, UNIT>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+  if (e != cudaSuccess) return e;
+  k_build_tiles<CntT, UNIT><<<grid, block, sm, st>>>(A);
+  return cudaGetLastError();
 }
 
 cudaError_t launch_build_tiles(const BuildArgs& A, int count_bits, int n_layers,
                                cudaStream_t st) {
-  dim3 grid((unsigned)A.tiles_per_layer, (unsigned)n_layers);
-  dim3 block((unsigned)(32 * A.P.na));
-  size_t sm = build_smem_bytes(A.P.na, A.P.nm, A.rc);
-  cudaError_t e;
-  if (count_bits == 16) {
-    e = cudaFuncSetAttribute(k_build_tiles<uint16_t>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)sm);
-    if (e != cudaSuccess) return e;
-    k_build_tiles<uint16_t><<<grid, block, sm, st>>>(A);
-  } else {
-    e = cudaFuncSetAttribute(k_build_tiles<uint32_t>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)sm);
-    if (e != cudaSuccess) return e;
-    k_build_tiles<uint32_t><<<grid, block, sm, st>>>(A);
-  }
-  return cudaGetLastError();
+  const bool unit = A.P.unit_step != 0;
+  if (count_bits == 16) return unit ? launch_one<uint16_t, true>(A, n_layers, st)
+                                    : launch_one<uint16_t, false>(A, n_layers, st);
+  return unit ? launch_one<uint32_t, true>(A, n_layers, st) : launch_one<uint32_t, false>(A, n_layers, st);
 }
 
 cudaError_t launch_scan_tiles(const int32_t* tile_len, int64_t n_tiles, int64_t* canon,
-                              int64_t* total, cudaStream_t st) {
-  k_scan_tiles<<<1, 1024, 0, st>>>(tile_len, n_tiles, canon, total);
+                              int64_t* total, int64_t* block_sums, cudaStream_t st) {
+  const int64_t nb = (n_tiles + kScanBlock - 1) / kScanBlock;
+  if (nb == 0) return cudaSuccess;
+  k_scan_sums<<<(unsigned)nb, kScanBlock, 0, st>>>(tile_len, n_tiles, block_sums);
+  k_scan_block_sums<<<1, 1024, 0, st>>>(block_sums, nb, total);
+  k_scan_finish<<<(unsigned)nb, kScanBlock, 0, st>>>(tile_len, n_tiles, block_sums, canon);
   return cudaGetLastError();
 }
 
 cudaError_t launch_assemble(const AssembleArgs& A, int count_bits, int index_bits,
                             cudaStream_t st) {
-  dim3 grid((unsigned)A.n_tiles), block(256);
+  dim3 grid((unsigned)((A.n_tiles + 7) / 8)), block(256);
   if (A.n_tiles == 0) return cudaSuccess;
   if (count_bits == 16 && index_bits == 32) k_assemble<uint16_t, int32_t><<<grid, block, 0, st>>>(A);
   else if (count_bits == 16) k_assemble<uint16_t, int64_t><<<grid, block, 0, st>>>(A);

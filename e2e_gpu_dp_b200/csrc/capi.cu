@@ -3,6 +3,7 @@
 
 #include <algorithm>
 #include <chrono>
+#include <mutex>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -37,6 +38,61 @@ e2e_status cuda_fail(cudaError_t e, const char* what) {
     cudaError_t _e = (call);                              \
     if (_e != cudaSuccess) return cuda_fail(_e, #call);   \
   } while (0)
+
+// ---------------------------------------------------------------------------------
+// device memory: one stream-ordered pool per device owned by the library.  Its
+// release threshold is unbounded, so memory freed by one build is reused by the
+// next without returning to the driver at every synchronisation (which made
+// repeated builds pay for re-mapping gigabytes); e2e_memory_trim releases it.
+// ---------------------------------------------------------------------------------
+namespace {
+std::mutex g_pool_mu;
+cudaMemPool_t g_pool[64] = {};
+}  // namespace
+
+namespace e2e {
+cudaError_t device_pool(cudaMemPool_t* out) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
+  std::lock_guard<std::mutex> lk(g_pool_mu);
+  if (!g_pool[dev]) {
+    cudaMemPoolProps props;
+    std::memset(&props, 0, sizeof(props));
+    props.allocType = cudaMemAllocationTypePinned;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = dev;
+    cudaMemPool_t pool;
+    e = cudaMemPoolCreate(&pool, &props);
+    if (e != cudaSuccess) return e;
+    uint64_t thr = UINT64_MAX;
+    e = cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
+    if (e != cudaSuccess) return e;
+    g_pool[dev] = pool;
+  }
+  *out = g_pool[dev];
+  return cudaSuccess;
+}
+
+cudaError_t dalloc(void** p, size_t bytes, cudaStream_t st) {
+  cudaMemPool_t pool;
+  cudaError_t e = device_pool(&pool);
+  if (e != cudaSuccess) return e;
+  return cudaMallocFromPoolAsync(p, bytes ? bytes : 16, pool, st);
+}
+}  // namespace e2e
+
+extern "C" e2e_status e2e_memory_trim(void) {
+  cudaMemPool_t pool;
+  cudaError_t e = device_pool(&pool);
+  if (e != cudaSuccess) return cuda_fail(e, "device_pool");
+  e = cudaDeviceSynchronize();
+  if (e != cudaSuccess) return cuda_fail(e, "cudaDeviceSynchronize");
+  e = cudaMemPoolTrimTo(pool, 0);
+  if (e != cudaSuccess) return cuda_fail(e, "cudaMemPoolTrimTo");
+  return E2E_OK;
+}
 
 extern "C" int e2e_abi_version(void) { return E2E_DP_ABI_VERSION; }
 
@@ -128,7 +184,7 @@ e2e_status validate_problem(const e2e_problem* p) {
     return fail(E2E_ERR_INVALID, "num_actions must equal num_ac_speeds * num_ac_angles");
   if (p->num_actions > 32) return fail(E2E_ERR_UNSUPPORTED, "at most 32 actions are supported");
   if (p->nrzns < 1) return fail(E2E_ERR_INVALID, "nrzns must be >= 1");
-  if (p->nrzns > 65535) return fail(E2E_ERR_UNSUPPORTED, "nrzns above 65535 is not supported");
+  if (p->nrzns > 32767) return fail(E2E_ERR_UNSUPPORTED, "nrzns above 32767 is not supported");
   if (p->nmodes < 0 || p->nmodes > 256) return fail(E2E_ERR_INVALID, "nmodes out of range");
   if (p->neighb_gsize < 1 || p->neighb_gsize % 2 != 1 || p->neighb_gsize > p->gsize)
     return fail(E2E_ERR_INVALID, "neighb_gsize must be odd and <= gsize (src/build_model.cu:1027-1028)");
@@ -178,7 +234,7 @@ e2e_status upload(const void* src, size_t bytes, int where, void** dst, bool* ow
     return E2E_OK;
   }
   void* d = nullptr;
-  CK(cudaMallocAsync(&d, bytes ? bytes : 16, st));
+  CK(dalloc((void**)&d, bytes ? bytes : 16, st));
   if (bytes) {
     cudaError_t e = cudaMemcpyAsync(d, src, bytes, cudaMemcpyHostToDevice, st);
     if (e != cudaSuccess) {
@@ -200,7 +256,7 @@ e2e_status make_dev_problem(const e2e_problem* p, cudaStream_t st, DevProblem* D
   const int g = p->gsize, na = p->num_actions;
   size_t bytes = sizeof(float) * (2 * (size_t)g + 4 * (size_t)na);
   float* d = nullptr;
-  CK(cudaMallocAsync((void**)&d, bytes, st));
+  CK(dalloc((void**)&d, bytes, st));
   keep->add(d);
   std::vector<float> h(2 * (size_t)g + 4 * (size_t)na);
   std::copy(xs.begin(), xs.end(), h.begin());
@@ -235,6 +291,8 @@ e2e_status make_dev_problem(const e2e_problem* p, cudaStream_t st, DevProblem* D
   D->Dj = std::fabs(xs[1] - xs[0]);
   D->Di = std::fabs(ys[1] - ys[0]);
   D->unit_step = (D->Dj == 1.0f && D->Di == 1.0f) ? 1 : 0;
+  D->axmax = xs[g - 1] - xs[0];
+  D->aymax = -(ys[0] - ys[g - 1]);
   D->xs = d;
   D->ys = d + g;
   D->ac_speed = d + 2 * g;
@@ -265,10 +323,11 @@ ViModel vi_model(const e2e_model* m) {
 }
 
 void free_model_buffers(e2e_model* m) {
-  if (m->row_ptr) cudaFree(m->row_ptr);
-  if (m->col) cudaFree(m->col);
-  if (m->cnt) cudaFree(m->cnt);
-  if (m->R) cudaFree(m->R);
+  // pool memory, released in stream order on the legacy default stream
+  if (m->row_ptr) cudaFreeAsync(m->row_ptr, 0);
+  if (m->col) cudaFreeAsync(m->col, 0);
+  if (m->cnt) cudaFreeAsync(m->cnt, 0);
+  if (m->R) cudaFreeAsync(m->R, 0);
   m->row_ptr = nullptr;
   m->col = nullptr;
   m->cnt = nullptr;
@@ -356,8 +415,13 @@ e2e_status plan_build(const e2e_problem* p, int count_bits, int64_t stage_hint, 
   pl->ns = pl->ncells * p->nt;
   pl->na = p->num_actions;
   pl->n_rows = (int64_t)(p->nt - 1) * pl->ncells * pl->na;
-  pl->tiles_per_layer = (pl->ncells + 31) / 32;
-  pl->n_tiles = pl->tiles_per_layer * (p->nt - 1);
+  pl->tiles_per_layer = (pl->ncells + 31) / 32;  // builder CTAs per layer
+  {
+    const int nwarps = 1 << build_lanes_log2(pl->na);  // emission tiles (warps) per CTA
+    pl->cells_per_tile = 32 / nwarps;
+    pl->etiles_per_layer = pl->tiles_per_layer * nwarps;
+    pl->n_tiles = pl->etiles_per_layer * (p->nt - 1);
+  }
   pl->rc = pl->na >= 16 ? 128 : 64;
   size_t sm = build_smem_bytes(pl->na, p->nmodes, pl->rc);
   while (sm > 200 * 1024 && pl->rc > 16) {
@@ -409,19 +473,19 @@ e2e_status run_build(const e2e_problem* p, const DevFields& F, const BuildPlan& 
   if (s != E2E_OK) return s;
   const int cbytes = pl.count_bits == 16 ? 2 : 4;
   // model R (state-major, last layer zero as src/build_model.cu:1173-1176)
-  CK(cudaMalloc((void**)&m->R, sizeof(float) * (size_t)pl.ns * pl.na));
+  CK(dalloc((void**)&m->R, sizeof(float) * (size_t)pl.ns * pl.na, st));
   CK(cudaMemsetAsync(m->R, 0, sizeof(float) * (size_t)pl.ns * pl.na, st));
   uint32_t* row_off = nullptr;
   int64_t* tile_base = nullptr;
   int32_t* tile_len = nullptr;
   unsigned long long* ctr = nullptr;
-  CK(cudaMallocAsync((void**)&row_off, sizeof(uint32_t) * (size_t)std::max<int64_t>(pl.n_rows, 1), st));
+  CK(dalloc((void**)&row_off, sizeof(uint32_t) * (size_t)std::max<int64_t>(pl.n_rows, 1), st));
   scratch->add(row_off);
-  CK(cudaMallocAsync((void**)&tile_base, sizeof(int64_t) * (size_t)std::max<int64_t>(pl.n_tiles, 1), st));
+  CK(dalloc((void**)&tile_base, sizeof(int64_t) * (size_t)std::max<int64_t>(pl.n_tiles, 1), st));
   scratch->add(tile_base);
-  CK(cudaMallocAsync((void**)&tile_len, sizeof(int32_t) * (size_t)std::max<int64_t>(pl.n_tiles, 1), st));
+  CK(dalloc((void**)&tile_len, sizeof(int32_t) * (size_t)std::max<int64_t>(pl.n_tiles, 1), st));
   scratch->add(tile_len);
-  CK(cudaMallocAsync((void**)&ctr, sizeof(unsigned long long) * CTR_COUNT, st));
+  CK(dalloc((void**)&ctr, sizeof(unsigned long long) * CTR_COUNT, st));
   scratch->add(ctr);
 
   int64_t cap = pl.stage_cap, pool_units = pl.pool_units;
@@ -438,10 +502,10 @@ e2e_status run_build(const e2e_problem* p, const DevFields& F, const BuildPlan& 
   } evfree{ev};
   for (int attempt = 0; attempt < 3; ++attempt) {
     if (!stage_col) {
-      CK(cudaMallocAsync((void**)&stage_col, sizeof(int32_t) * (size_t)cap, st));
-      CK(cudaMallocAsync(&stage_cnt, (size_t)cbytes * (size_t)cap, st));
+      CK(dalloc((void**)&stage_col, sizeof(int32_t) * (size_t)cap, st));
+      CK(dalloc((void**)&stage_cnt, (size_t)cbytes * (size_t)cap, st));
     }
-    if (!pool) CK(cudaMallocAsync((void**)&pool, sizeof(uint32_t) * (size_t)mm * (size_t)pool_units, st));
+    if (!pool) CK(dalloc((void**)&pool, sizeof(uint32_t) * (size_t)mm * (size_t)pool_units, st));
     CK(cudaMemsetAsync(ctr, 0, sizeof(unsigned long long) * CTR_COUNT, st));
     BuildArgs A;
     A.P = D;
@@ -449,6 +513,7 @@ e2e_status run_build(const e2e_problem* p, const DevFields& F, const BuildPlan& 
     A.t0 = 0;
     A.tiles_per_layer = (int)pl.tiles_per_layer;
     A.rc = pl.rc;
+    A.lanes_log2 = build_lanes_log2(pl.na);
     A.stage_col = stage_col;
     A.stage_cnt = stage_cnt;
     A.stage_cap = cap;
@@ -506,20 +571,24 @@ e2e_status run_build(const e2e_problem* p, const DevFields& F, const BuildPlan& 
   m->prob = *p;
   m->has_prob = true;
   const int pb = m->index_bits == 32 ? 4 : 8;
-  CK(cudaMalloc(&m->row_ptr, (size_t)pb * (size_t)(pl.n_rows + 1)));
-  CK(cudaMalloc((void**)&m->col, sizeof(int32_t) * (size_t)std::max<int64_t>(nnz, 1)));
-  CK(cudaMalloc(&m->cnt, (size_t)cbytes * (size_t)std::max<int64_t>(nnz, 1)));
+  CK(dalloc(&m->row_ptr, (size_t)pb * (size_t)(pl.n_rows + 1), st));
+  CK(dalloc((void**)&m->col, sizeof(int32_t) * (size_t)(nnz + 16), st));
+  CK(dalloc(&m->cnt, (size_t)cbytes * (size_t)(nnz + 16), st));
   int64_t* canon = nullptr;
   int64_t* total = nullptr;
-  CK(cudaMallocAsync((void**)&canon, sizeof(int64_t) * (size_t)std::max<int64_t>(pl.n_tiles, 1), st));
+  CK(dalloc((void**)&canon, sizeof(int64_t) * (size_t)std::max<int64_t>(pl.n_tiles, 1), st));
   scratch->add(canon);
-  CK(cudaMallocAsync((void**)&total, sizeof(int64_t), st));
+  CK(dalloc((void**)&total, sizeof(int64_t), st));
   scratch->add(total);
   CK(cudaEventRecord(ev[2], st));
-  CK(launch_scan_tiles(tile_len, pl.n_tiles, canon, total, st));
+  int64_t* block_sums = nullptr;
+  CK(dalloc((void**)&block_sums, sizeof(int64_t) * (size_t)(pl.n_tiles / 1024 + 2), st));
+  scratch->add(block_sums);
+  CK(launch_scan_tiles(tile_len, pl.n_tiles, canon, total, block_sums, st));
   AssembleArgs S;
   S.n_tiles = pl.n_tiles;
-  S.tiles_per_layer = pl.tiles_per_layer;
+  S.tiles_per_layer = pl.etiles_per_layer;
+  S.cells_per_tile = pl.cells_per_tile;
   S.ncells = pl.ncells;
   S.n_rows = pl.n_rows;
   S.total_nnz = nnz;
@@ -622,9 +691,9 @@ e2e_status solve_on_device(const e2e_model* m, const e2e_vi_opts& o, float* dV, 
   float* W = nullptr;
   unsigned long long* resid = nullptr;
   const int max_iter = o.max_iter > 0 ? o.max_iter : (m->nt > 0 ? m->nt + 2 : 100000);
-  CK(cudaMallocAsync((void**)&W, sizeof(float) * (size_t)ns, st));
+  CK(dalloc((void**)&W, sizeof(float) * (size_t)ns, st));
   scratch.add(W);
-  CK(cudaMallocAsync((void**)&resid, sizeof(unsigned long long) * (size_t)(max_iter + 2), st));
+  CK(dalloc((void**)&resid, sizeof(unsigned long long) * (size_t)(max_iter + 2), st));
   scratch.add(resid);
   CK(cudaMemsetAsync(resid, 0, sizeof(unsigned long long) * (size_t)(max_iter + 2), st));
   cudaEvent_t e0, e1;
@@ -651,7 +720,7 @@ e2e_status solve_on_device(const e2e_model* m, const e2e_vi_opts& o, float* dV, 
       CK(launch_vi_sweep(M, t * nc, (t + 1) * nc, dV, dV, dpi, nullptr, st));
     // verification sweep (Jacobi from the fixed point): residual must be 0
     int32_t* pi2 = nullptr;
-    CK(cudaMallocAsync((void**)&pi2, sizeof(int32_t) * (size_t)ns, st));
+    CK(dalloc((void**)&pi2, sizeof(int32_t) * (size_t)ns, st));
     scratch.add(pi2);
     CK(launch_vi_sweep(M, 0, ns, dV, W, pi2, resid, st));
     unsigned long long h = 0;
@@ -710,9 +779,9 @@ e2e_status solve_on_device(const e2e_model* m, const e2e_vi_opts& o, float* dV, 
     if (!m->layered) return fail(E2E_ERR_UNSUPPORTED, "fp64 check needs a time-layered model");
     double* Vd = nullptr;
     unsigned long long* err = nullptr;
-    CK(cudaMallocAsync((void**)&Vd, sizeof(double) * (size_t)ns, st));
+    CK(dalloc((void**)&Vd, sizeof(double) * (size_t)ns, st));
     scratch.add(Vd);
-    CK(cudaMallocAsync((void**)&err, sizeof(unsigned long long) * 2, st));
+    CK(dalloc((void**)&err, sizeof(unsigned long long) * 2, st));
     scratch.add(err);
     CK(cudaMemsetAsync(err, 0, sizeof(unsigned long long) * 2, st));
     const int64_t nc = m->ncells;
@@ -754,13 +823,13 @@ extern "C" e2e_status e2e_spvi_solve(const e2e_model* m, const e2e_vi_opts* opts
   if (out_where == E2E_DEVICE && value_out) {
     dV = value_out;
   } else {
-    CK(cudaMallocAsync((void**)&dV, sizeof(float) * (size_t)ns, st));
+    CK(dalloc((void**)&dV, sizeof(float) * (size_t)ns, st));
     scratch.add(dV);
   }
   if (out_where == E2E_DEVICE && policy_out) {
     dpi = policy_out;
   } else {
-    CK(cudaMallocAsync((void**)&dpi, sizeof(int32_t) * (size_t)ns, st));
+    CK(dalloc((void**)&dpi, sizeof(int32_t) * (size_t)ns, st));
     scratch.add(dpi);
   }
   e2e_status s = solve_on_device(m, o, dV, dpi, stats, st);

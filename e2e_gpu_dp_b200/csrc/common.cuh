@@ -29,6 +29,7 @@ struct DevProblem {
   float dt, r_out, r_term, alpha;
   float xs0, xsn, ys0, ysn;  // xs[0], xs[g-1], ys[0], ys[g-1]
   float Dj, Di;              // fabsf(xs[1]-xs[0]), fabsf(ys[1]-ys[0])
+  float axmax, aymax;        // xsn - xs0 and -(ys0 - ysn): snapping-coordinate bounds
   const float* xs;           // device, g
   const float* ys;           // device, g
   const float* ac_speed;     // device, na
@@ -71,35 +72,22 @@ __device__ __forceinline__ float step_reward(const DevProblem& P, float ac_speed
     return 0;
 }
 
-// move(), src/build_model.cu:268-356: advect one step, clamp to the domain,
-// snap to the nearest cell centre, add edge / terminal / late-time rewards.
-// (x, y) is the centre of the start cell; on return (i2, j2) is the next cell.
-__device__ __forceinline__ void move_sample(const DevProblem& P, float F, float cs, float sn,
-                                            float vx, float vy, float x, float y, bool late,
-                                            int& i2, int& j2, float& r) {
+// Advection of move(), src/build_model.cu:284-289: the reference's expressions.
+__device__ __forceinline__ void advect(const DevProblem& P, float F, float cs, float sn, float vx,
+                                      float vy, float x, float y, float& xnew, float& ynew) {
   float vnetx = F * cs + vx;
   float vnety = F * sn + vy;
-  float xnew = x + (vnetx * P.dt);
-  float ynew = y + (vnety * P.dt);
-  r = 0;
-  if (xnew > P.xsn) {
-    xnew = P.xsn;
-    r += P.r_out;
-  } else if (xnew < P.xs0) {
-    xnew = P.xs0;
-    r += P.r_out;
-  }
-  if (ynew > P.ysn) {
-    ynew = P.ysn;
-    r += P.r_out;
-  } else if (ynew < P.ys0) {
-    ynew = P.ys0;
-    r += P.r_out;
-  }
-  int32_t xind, yind;
-  if (P.unit_step) {
-    // remainderf(a, 1) == a - rintf(a) exactly, and (a - rem)/1 == rintf(a);
-    // the reference's round-half-up (rem >= 0.5) is applied on top.
+  xnew = x + (vnetx * P.dt);
+  ynew = y + (vnety * P.dt);
+}
+
+// Snapping of move(), src/build_model.cu:313-335: nearest cell centre with
+// ties rounded up.  UNIT (Dj == Di == 1): remainderf(a, 1) == a - rintf(a)
+// exactly and (a - rem)/1 == rintf(a), so rintf gives the same indices.
+template <bool UNIT>
+__device__ __forceinline__ void snap(const DevProblem& P, float xnew, float ynew, int32_t& xind,
+                                     int32_t& yind) {
+  if (UNIT) {
     float ax = xnew - P.xs0;
     float ay = -(ynew - P.ysn);
     float nx = rintf(ax);
@@ -116,6 +104,34 @@ __device__ __forceinline__ void move_sample(const DevProblem& P, float F, float 
     if (remx >= 0.5 * P.Dj) xind += 1;
     if (remy >= 0.5 * P.Di) yind += 1;
   }
+}
+
+// move(), src/build_model.cu:268-356: advect one step, clamp to the domain,
+// snap to the nearest cell centre, add edge / terminal / late-time rewards.
+// (x, y) is the centre of the start cell; on return (i2, j2) is the next cell.
+template <bool UNIT>
+__device__ __forceinline__ void move_sample(const DevProblem& P, float F, float cs, float sn,
+                                            float vx, float vy, float x, float y, bool late,
+                                            int& i2, int& j2, float& r) {
+  float xnew, ynew;
+  advect(P, F, cs, sn, vx, vy, x, y, xnew, ynew);
+  r = 0;
+  if (xnew > P.xsn) {
+    xnew = P.xsn;
+    r += P.r_out;
+  } else if (xnew < P.xs0) {
+    xnew = P.xs0;
+    r += P.r_out;
+  }
+  if (ynew > P.ysn) {
+    ynew = P.ysn;
+    r += P.r_out;
+  } else if (ynew < P.ys0) {
+    ynew = P.ys0;
+    r += P.r_out;
+  }
+  int32_t xind, yind;
+  snap<UNIT>(P, xnew, ynew, xind, yind);
   i2 = yind;
   j2 = xind;
   int32_t n = P.g - 1;
@@ -125,6 +141,59 @@ __device__ __forceinline__ void move_sample(const DevProblem& P, float F, float 
   } else {
     if (late) r += 0.05 * P.r_out;
   }
+}
+
+// The landing cell of move_sample without the rewards, for unit cell spacing.
+//
+// The clamps of move() are applied to the snapping coordinates instead:
+// ax = xnew - xs0 clamped to [0, xsn - xs0] and ay = -(ynew - ysn) clamped to
+// [0, -(ys0 - ysn)].  Rounding is monotone, so inside the domain the values
+// are the reference's, beyond an edge they equal the reference's clamped
+// values, and a NaN becomes 0 (fmaxf returns the non-NaN operand), which is
+// the index the reference's float-to-int conversion gives a NaN.
+//
+// Index: the reference takes n = rint(a) (remainderf with spacing 1) and adds
+// 1 when a - n >= 0.5, i.e. it rounds half up: index = floor(a + 0.5), exactly.
+// With round-toward-minus-infinity adds, w = RD(a + 0.5) has floor(w) ==
+// floor(a + 0.5) (integers below 2^24 are floats, so w cannot drop below it),
+// and RD(w + 1.5*2^23) == 1.5*2^23 + floor(w) because floats in [2^23, 2^24)
+// are spaced by 1; the integer is then the low mantissa bits.
+__device__ __forceinline__ int32_t round_half_up_index(float a, int32_t bias) {
+  const float w = __fadd_rd(a, 0.5f);
+  const float t = __fadd_rd(w, 12582912.0f);  // 1.5 * 2^23
+  return __float_as_int(t) - bias;            // bias = bits of 1.5*2^23 (+ window origin)
+}
+
+__device__ __forceinline__ void land_unit(const DevProblem& P, float F, float cs, float sn,
+                                          float vx, float vy, float x, float y, int& i2, int& j2) {
+  float xnew, ynew;
+  advect(P, F, cs, sn, vx, vy, x, y, xnew, ynew);
+  const float ax = fminf(fmaxf(xnew - P.xs0, 0.0f), P.axmax);
+  const float ay = fminf(fmaxf(-(ynew - P.ysn), 0.0f), P.aymax);
+  j2 = round_half_up_index(ax, 0x4B400000);
+  i2 = round_half_up_index(ay, 0x4B400000);
+}
+
+// General spacing: the reference's clamps (if / else) and remainderf snap.
+__device__ __forceinline__ void land_general(const DevProblem& P, float F, float cs, float sn,
+                                             float vx, float vy, float x, float y, int& i2, int& j2) {
+  float xnew, ynew;
+  advect(P, F, cs, sn, vx, vy, x, y, xnew, ynew);
+  if (xnew > P.xsn) xnew = P.xsn;
+  else if (xnew < P.xs0) xnew = P.xs0;
+  if (ynew > P.ysn) ynew = P.ysn;
+  else if (ynew < P.ys0) ynew = P.ys0;
+  int32_t xind, yind;
+  snap<false>(P, xnew, ynew, xind, yind);
+  i2 = yind;
+  j2 = xind;
+}
+
+template <bool UNIT>
+__device__ __forceinline__ void land(const DevProblem& P, float F, float cs, float sn, float vx,
+                                     float vy, float x, float y, int& i2, int& j2) {
+  if (UNIT) land_unit(P, F, cs, sn, vx, vy, x, y, i2, j2);
+  else land_general(P, F, cs, sn, vx, vy, x, y, i2, j2);
 }
 
 __device__ __forceinline__ bool is_terminal(const DevProblem& P, int i, int j) {

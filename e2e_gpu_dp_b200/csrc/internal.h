@@ -33,6 +33,8 @@ struct e2e_model {
 namespace e2e {
 
 e2e_status fail(e2e_status st, const std::string& msg);
+// device allocation from the library's stream-ordered pool (free with cudaFreeAsync)
+cudaError_t dalloc(void** p, size_t bytes, cudaStream_t st);
 e2e_status cuda_fail(cudaError_t e, const char* what);
 
 // Stream-ordered temporaries released when the owner goes out of scope.
@@ -53,6 +55,7 @@ struct DeviceScratch {
 struct BuildPlan {
   int count_bits = 16;
   int64_t ncells = 0, ns = 0, n_rows = 0, tiles_per_layer = 0, n_tiles = 0;
+  int64_t etiles_per_layer = 0, cells_per_tile = 32;  // emission tiles (one per builder warp)
   int na = 0, rc = 128;
   int64_t stage_cap = 0, pool_units = 0;
 };

@@ -25,8 +25,9 @@ struct BuildArgs {
   DevProblem P;
   DevFields F;
   int t0;               // first layer of this launch (blockIdx.y offset)
-  int tiles_per_layer;  // ceil(ncells / 32)
-  int rc;               // realisations per shared-memory chunk
+  int tiles_per_layer;  // CTAs per layer = ceil(ncells / 32); emission tiles are warps
+  int rc;               // (unused) realisations per chunk
+  int lanes_log2;       // lanes per cell = 1 << lanes_log2 >= na
   int32_t* stage_col;
   void* stage_cnt;
   int64_t stage_cap;
@@ -40,7 +41,7 @@ struct BuildArgs {
 };
 
 struct AssembleArgs {
-  int64_t n_tiles, tiles_per_layer, ncells, n_rows, total_nnz;
+  int64_t n_tiles, tiles_per_layer, cells_per_tile, ncells, n_rows, total_nnz;
   int na;
   const int64_t* tile_base;
   const int32_t* tile_len;
@@ -53,10 +54,11 @@ struct AssembleArgs {
   void* cnt;
 };
 
+int build_lanes_log2(int na);
 size_t build_smem_bytes(int na, int nm, int rc);
 cudaError_t launch_build_tiles(const BuildArgs& A, int count_bits, int n_layers, cudaStream_t st);
 cudaError_t launch_scan_tiles(const int32_t* tile_len, int64_t n_tiles, int64_t* canon,
-                              int64_t* total, cudaStream_t st);
+                              int64_t* total, int64_t* block_sums, cudaStream_t st);
 cudaError_t launch_assemble(const AssembleArgs& A, int count_bits, int index_bits,
                             cudaStream_t st);
 cudaError_t launch_action_trig(const float* angle, int n, float* cosv, float* sinv,

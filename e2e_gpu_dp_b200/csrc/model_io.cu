@@ -212,9 +212,9 @@ extern "C" e2e_status e2e_model_read_npy(const char* dir, e2e_model** out, void*
   };
   cudaError_t e;
   const size_t pb = m->index_bits == 32 ? 4 : 8;
-  if ((e = cudaMalloc(&m->row_ptr, pb * rp.size())) != cudaSuccess) return cleanup(E2E_OK, e, "cudaMalloc(row_ptr)");
-  if ((e = cudaMalloc((void**)&m->col, 4 * col.size())) != cudaSuccess) return cleanup(E2E_OK, e, "cudaMalloc(col)");
-  if ((e = cudaMalloc((void**)&m->R, 4 * Rsa.size())) != cudaSuccess) return cleanup(E2E_OK, e, "cudaMalloc(R)");
+  if ((e = dalloc(&m->row_ptr, pb * rp.size(), st)) != cudaSuccess) return cleanup(E2E_OK, e, "alloc(row_ptr)");
+  if ((e = dalloc((void**)&m->col, 4 * (col.size() + 16), st)) != cudaSuccess) return cleanup(E2E_OK, e, "alloc(col)");
+  if ((e = dalloc((void**)&m->R, 4 * Rsa.size(), st)) != cudaSuccess) return cleanup(E2E_OK, e, "alloc(R)");
   if (m->index_bits == 32) {
     std::vector<int32_t> rp32(rp.begin(), rp.end());
     e = cudaMemcpyAsync(m->row_ptr, rp32.data(), 4 * rp32.size(), cudaMemcpyHostToDevice, st);
@@ -230,11 +230,11 @@ extern "C" e2e_status e2e_model_read_npy(const char* dir, e2e_model** out, void*
   if (m->count_type == E2E_COUNT_U16) {
     std::vector<uint16_t> c16((size_t)std::max<int64_t>(nnz, 1));
     for (int64_t k = 0; k < nnz; ++k) c16[(size_t)k] = (uint16_t)std::rint((double)v[(size_t)k] * m->nrzns);
-    if ((e = cudaMalloc(&m->cnt, 2 * c16.size())) != cudaSuccess) return cleanup(E2E_OK, e, "cudaMalloc(cnt)");
+    if ((e = dalloc(&m->cnt, 2 * (c16.size() + 16), st)) != cudaSuccess) return cleanup(E2E_OK, e, "alloc(cnt)");
     e = cudaMemcpyAsync(m->cnt, c16.data(), 2 * c16.size(), cudaMemcpyHostToDevice, st);
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);
   } else {
-    if ((e = cudaMalloc(&m->cnt, 4 * v.size())) != cudaSuccess) return cleanup(E2E_OK, e, "cudaMalloc(cnt)");
+    if ((e = dalloc(&m->cnt, 4 * (v.size() + 16), st)) != cudaSuccess) return cleanup(E2E_OK, e, "alloc(cnt)");
     e = cudaMemcpyAsync(m->cnt, v.data(), 4 * v.size(), cudaMemcpyHostToDevice, st);
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);
   }

@@ -157,6 +157,12 @@ const char* e2e_status_string(e2e_status st);
 /* Message of the last failure on the calling host thread ("" if none). */
 const char* e2e_last_error(void);
 
+/* Release the device memory the library keeps cached for later builds and
+ * solves (its stream-ordered pool never returns memory on its own).  Waits for
+ * the device.  No counterpart in the reference, whose thrust vectors allocate
+ * and free per (t, a). */
+e2e_status e2e_memory_trim(void);
+
 /* prob_params.npy slots <-> e2e_problem (src/build_model.cu:1032-1055). */
 e2e_status e2e_problem_from_params(const float prob_params[32], e2e_problem* out);
 e2e_status e2e_problem_to_params(const e2e_problem* p, float prob_params_out[32]);
