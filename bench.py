@@ -230,7 +230,11 @@ def run_ours(args, ws, rank, local):
     k1_ms = statistics.mean(r[0]["build_kernel_ms"] for r in recs)
     asm_ms = statistics.mean(r[0]["assemble_ms"] for r in recs)
     solve_ms = statistics.mean(r[1]["seconds"] * 1e3 for r in recs)
-    launches = 4 + (prob.nt + 1)  # trig, build, scan, assemble; last layer + nt-1 layers + verification
+    pack_ms = statistics.mean(r[1]["pack_ms"] for r in recs)
+    pass_ms = statistics.mean(r[1]["sweep_seconds"] * 1e3 for r in recs)
+    # trig, build, 3 scan kernels, assemble; pack count, 3 scan kernels, pack fill;
+    # the persistent layered sweep and the verification sweep
+    launches = 6 + 5 + 2
 
     # e2e through the C ABI from pinned host memory
     pinned = {k: torch.from_numpy(np.ascontiguousarray(v)).pin_memory() for k, v in fields.items()}
@@ -266,7 +270,8 @@ def run_ours(args, ws, rank, local):
     _, _, lst = m.solve(method="layered", fp64_check=True, value=V, policy=pi, stream=stream)
     m.free()
     hbm, peak_kind = _peaks()
-    vi_gbs = jst["bytes_per_sweep"] * jst["iterations"] / jst["seconds"] / 1e9
+    vi_gbs = jst["stream_bytes_per_sweep"] * jst["iterations"] / jst["seconds"] / 1e9
+    vi_csr_gbs = jst["bytes_per_sweep"] * jst["iterations"] / jst["seconds"] / 1e9
 
     cb = 2 if info["count_type"] == 0 else 4
     k1_bytes = algorithmic_build_bytes(prob, info["nnz"], cb)
@@ -305,23 +310,249 @@ def run_ours(args, ws, rank, local):
                 "d2h_bytes_per_step": d2h},
         "gpu_launches": launches,
         "phases_ms": {"build_kernel": round(k1_ms, 3), "assemble": round(asm_ms, 3),
-                      "solve": round(solve_ms, 3)},
+                      "pack": round(pack_ms, 3), "solve": round(solve_ms, 3),
+                      "layered_pass": round(pass_ms, 3)},
         "roofline": {"kernel": "k_build_tiles", "bound": "hbm", "achieved": round(k1_gbs, 2),
                      "peak": hbm, "unit": "GB/s", "frac": round(k1_gbs / hbm, 5),
                      "traffic": traffic, "peak_source": f"{peak_kind} hbm_gbs",
                      "algorithmic_bytes": k1_bytes,
                      "note": "issue-bound Monte-Carlo kernel; samples/s is its throughput"},
         "build_samples_per_s": round(samples / (k1_ms * 1e-3), 1),
-        "vi": {"kernel": "k_vi_sweep (Jacobi, reference schedule)", "iterations": jst["iterations"],
-               "bytes_per_sweep": jst["bytes_per_sweep"], "seconds": round(jst["seconds"], 6),
+        "vi": {"kernel": "k_vi_chunks (Jacobi, reference schedule)", "iterations": jst["iterations"],
+               "stream_bytes_per_sweep": jst["stream_bytes_per_sweep"],
+               "csr_bytes_per_sweep": jst["bytes_per_sweep"], "seconds": round(jst["seconds"], 6),
                "achieved_gbs": round(vi_gbs, 1), "frac": round(vi_gbs / hbm, 4),
+               "csr_equivalent_gbs": round(vi_csr_gbs, 1),
                "layered_seconds": round(lst["seconds"], 6),
+               "layered_pass_seconds": round(lst["sweep_seconds"], 6),
                "fp64_max_rel_err": lst["fp64_max_rel_err"]},
         "clocks": clocks,
     }
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(prob, fields, threads=os.cpu_count() or 1)
     return line
+
+
+def run_batched(n_models: int = 256, seed: int = 2024) -> dict:
+    """Batched form: ``n_models`` uneven planning problems (grid 32-160, nt
+    20-100, 8/16 headings, nrzns 200-2000, 4-8 modes, 0-5% obstacles, random
+    targets; one seed), built and solved one at a time through the plain API
+    (build_model + layered solve + free), and batched: groups of 32 built
+    concurrently and each group solved in one persistent launch.  Then the
+    solves alone with all models resident: one launch for all of them against
+    the plain solve of one model at a time.  Device-resident seeded fields;
+    times are CUDA events on the stream (or wall clock where larger)."""
+    import torch
+
+    from e2e_gpu_dp_b200 import api
+    from e2e_gpu_dp_b200.workloads import batch_instances, device_fields
+
+    insts = batch_instances(n_models, seed=seed)
+    stream = torch.cuda.current_stream()
+    fields = [device_fields(x.prob, x.spec) for x in insts]
+    outs = [(torch.empty(x.prob.ns, dtype=torch.float32, device="cuda"),
+             torch.empty(x.prob.ns, dtype=torch.int32, device="cuda")) for x in insts]
+    torch.cuda.synchronize()
+    ev = lambda: torch.cuda.Event(enable_timing=True)  # noqa: E731
+
+    # one warm-up problem for both arms (module loading, pool growth)
+    m = api.build_model(insts[0].prob, fields[0], stream=stream)
+    m.solve(method="layered", value=outs[0][0], policy=outs[0][1], stream=stream)
+    m.free()
+
+    # sequential: build, solve, free, one problem at a time
+    solve_s = 0.0
+    a, b = ev(), ev()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    a.record(stream)
+    for x, f, (V, pi) in zip(insts, fields, outs):
+        m = api.build_model(x.prob, f, stream=stream)
+        _, _, st = m.solve(method="layered", value=V, policy=pi, stream=stream)
+        solve_s += st["seconds"] + st["pack_ms"] * 1e-3
+        m.free()
+    b.record(stream)
+    torch.cuda.synchronize()
+    seq_s = max(a.elapsed_time(b) / 1e3, time.perf_counter() - t0)
+    ref = [(V.clone(), pi.clone()) for V, pi in outs]
+
+    # batched, pipelined: groups of 32 built concurrently (4 host threads, one
+    # stream each), each group solved in one launch, then freed
+    group = 32
+    for V, pi in outs:
+        V.fill_(float("nan"))
+        pi.fill_(-7)
+    a, c = ev(), ev()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    a.record(stream)
+    b_build = 0.0
+    first = None
+    for g0 in range(0, n_models, group):
+        tb = time.perf_counter()
+        models = api.build_models([x.prob for x in insts[g0:g0 + group]], fields[g0:g0 + group], workers=4)
+        b_build += time.perf_counter() - tb
+        st1 = api.solve_batch(models, [o[0] for o in outs[g0:g0 + group]], [o[1] for o in outs[g0:g0 + group]],
+                              stream=stream)
+        first = first or st1
+        for mm in models:
+            mm.free()
+    c.record(stream)
+    torch.cuda.synchronize()
+    total_s = max(a.elapsed_time(c) / 1e3, time.perf_counter() - t0)
+    same = all(torch.equal(V, r[0]) and torch.equal(pi, r[1]) for (V, pi), r in zip(outs, ref))
+
+    # solves alone, all models resident (built untimed): one batched launch
+    # (graph replay, tuned schedule) vs the plain API one model at a time
+    models = api.build_models([x.prob for x in insts], fields, workers=4)
+    api.solve_batch(models, [o[0] for o in outs], [o[1] for o in outs], stream=stream)
+    reps = []
+    for _ in range(5):
+        st2 = api.solve_batch(models, [o[0] for o in outs], [o[1] for o in outs], stream=stream)
+        reps.append(st2["seconds"])
+    same = same and all(torch.equal(V, r[0]) and torch.equal(pi, r[1]) for (V, pi), r in zip(outs, ref))
+    seq_solve_only = []
+    a, b = ev(), ev()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    a.record(stream)
+    for mm, (V, pi) in zip(models, outs):
+        _, _, st = mm.solve(method="layered", value=V, policy=pi, stream=stream)
+        seq_solve_only.append(st["sweep_seconds"])
+    b.record(stream)
+    torch.cuda.synchronize()
+    seq_resident_s = max(a.elapsed_time(b) / 1e3, time.perf_counter() - t0)
+    for mm in models:
+        mm.free()
+    rows = sum((x.prob.nt - 1) * x.prob.ncells * x.prob.num_actions for x in insts)
+    batch_solve_s = statistics.median(reps)
+    return {
+        "workload": f"{n_models} uneven MDPs: grid 32-160, nt 20-100, 8/16 headings, nrzns 200-2000, "
+                    "4-8 modes, 0-5% obstacles, random start/target, seed " + str(seed),
+        "models": n_models, "states": int(sum(x.prob.ns for x in insts)), "rows": int(rows),
+        "sequential_s": round(seq_s, 4), "sequential_solves_s": round(solve_s, 5),
+        "batched_total_s": round(total_s, 4), "batched_build_wall_s": round(b_build, 4),
+        "batched_group": group, "build_workers": 4,
+        "first_group_tune_ms": round(first["tune_ms"], 2),
+        "batched_solve_s": round(batch_solve_s, 6),
+        "sequential_resident_solves_s": round(seq_resident_s, 5),
+        "sequential_layered_passes_s": round(sum(seq_solve_only), 6),
+        "solves_per_s_batched": round(n_models / batch_solve_s, 1),
+        "solves_per_s_sequential": round(n_models / seq_resident_s, 1),
+        "solve_speedup_vs_sequential": round(seq_resident_s / batch_solve_s, 2),
+        "total_speedup_vs_sequential": round(seq_s / total_s, 3),
+        "schedule": {"warps_per_chunk": st2["groups"], "tune": st2["tune"], "ctas": st2["grid"],
+                     "graph": st2["graph"]},
+        "sweep_gbs": round(st2["stream_bytes"] / batch_solve_s / 1e9, 1),
+        "identical_to_sequential": bool(same),
+    }
+
+
+def run_served(rates=(50, 200, 500, 1000, 2000), seconds_per_rate=10.0, max_requests=20000,
+               plain_sample=40) -> dict:
+    """Served form: 16 resident fields (15 size classes drawn like the batched
+    form plus one 300x300x150 class), Poisson request streams (each request picks
+    a field, 8 or 16 headings, a target and a start; 2% pick the large field)
+    at each rate for ``seconds_per_rate`` (at most ``max_requests``), through the
+    request server; then a burst of requests submitted at once (capacity).  The
+    plain path - build the model with the request's target, solve, free - is
+    timed one request at a time on a sample of the same stream, and the served
+    values at the start cells are compared with it."""
+    import threading
+
+    import torch
+
+    from e2e_gpu_dp_b200 import api
+    from e2e_gpu_dp_b200.workloads import Request, device_fields, request_stream, serve_fields, with_target
+
+    fcs = serve_fields(16, n_large=1)
+    dev = [device_fields(fc.prob, fc.spec) for fc in fcs]
+    srv = api.Server(max_batch=256)
+    fids = [srv.add_field(fc.prob, f) for fc, f in zip(fcs, dev)]
+    assert fids == list(range(len(fcs)))
+
+    def serve(reqs, paced=True):
+        lat, qd, bs = [], [], []
+        results = {}
+
+        def submitter():
+            t0 = time.perf_counter()
+            for k, r in enumerate(reqs):
+                if paced:
+                    dt = t0 + r.arrival_s - time.perf_counter()
+                    if dt > 0:
+                        time.sleep(dt)
+                srv.submit(r.fid, r.headings, r.target, r.start, tag=k)
+        th = threading.Thread(target=submitter)
+        t0 = time.perf_counter()
+        th.start()
+        while len(results) < len(reqs):
+            for res in srv.poll(4096, wait_s=0.05):
+                results[res["tag"]] = res
+        t1 = time.perf_counter()
+        th.join()
+        for res in results.values():
+            lat.append(res["latency_ms"])
+            qd.append(res["queue_ms"])
+            bs.append(res["batch_size"])
+        fails = sum(1 for res in results.values() if res["status"] != 0)
+        return results, {"requests": len(reqs), "failed": fails, "seconds": round(t1 - t0, 4),
+                         "solves_per_s": round(len(reqs) / (t1 - t0), 1),
+                         "p50_ms": round(float(np.percentile(lat, 50)), 3),
+                         "p99_ms": round(float(np.percentile(lat, 99)), 3),
+                         "mean_queue_ms": round(float(np.mean(qd)), 3),
+                         "mean_batch": round(float(np.mean(bs)), 1), "max_batch": int(np.max(bs))}
+
+    # warm-up: every (field, heading set) base model built once (resident afterwards)
+    t0 = time.perf_counter()
+    warm = [Request(0.0, fid, h, (1, 1), (0, 0)) for fid in range(len(fcs)) for h in (8, 16)]
+    serve(warm, paced=False)
+    warm_s = time.perf_counter() - t0
+
+    per_rate = []
+    for lam in rates:
+        n = int(min(max_requests, lam * seconds_per_rate))
+        reqs = request_stream(fcs, n, lam, seed=int(lam))
+        _, stats = serve(reqs)
+        stats["rate"] = lam
+        per_rate.append(stats)
+    burst_reqs = request_stream(fcs, 5000, 1e9, seed=99)
+    burst_res, burst = serve(burst_reqs, paced=False)
+
+    # plain path on a sample of the burst's requests, one at a time
+    sample = burst_reqs[:plain_sample]
+    plain_lat, err = [], 0.0
+    torch.cuda.synchronize()
+    tp0 = time.perf_counter()
+    for k, r in enumerate(sample):
+        fc = fcs[r.fid]
+        ts = time.perf_counter()
+        m = api.build_model(with_target(fc.prob, r.headings, r.target), dev[r.fid])
+        V, pi, _ = m.solve(method="layered")
+        m.free()
+        plain_lat.append((time.perf_counter() - ts) * 1e3)
+        s0 = r.start[0] * fc.prob.gsize + r.start[1]
+        sv = burst_res[k]["value_at_start"]
+        err = max(err, abs(float(sv) - float(V[s0])) / max(1.0, abs(float(V[s0]))))
+    plain_s = time.perf_counter() - tp0
+    st = srv.stats()
+    srv.close()
+    plain_rate = len(sample) / plain_s
+    return {
+        "workload": "16 resident fields (15 of grid 32-160, nt 20-100, nrzns 200-2000, 4-8 modes; one "
+                    "300x300x150, nrzns 2000, 8 modes), 8/16 headings per request, random start/target, "
+                    "2% of requests on the large field; Poisson arrivals",
+        "warmup_builds_s": round(warm_s, 3), "models_resident": st["models_resident"],
+        "rates": per_rate, "burst": burst,
+        "plain": {"sample": len(sample), "solves_per_s": round(plain_rate, 2),
+                  "p50_ms": round(float(np.percentile(plain_lat, 50)), 3),
+                  "p99_ms": round(float(np.percentile(plain_lat, 99)), 3)},
+        "speedup_vs_plain_burst": round(burst["solves_per_s"] / plain_rate, 1),
+        "speedup_vs_plain_at_2000": round(per_rate[-1]["solves_per_s"] / plain_rate, 1),
+        "max_rel_value_err_vs_plain": err,
+        "server": {"batches": st["batches"], "models_built": st["models_built"],
+                   "bytes_in_use": st["bytes_in_use"], "device_solve_ms": round(st["solve_ms"], 2)},
+    }
 
 
 def run_reference(args, ws, rank, local):
@@ -401,7 +632,9 @@ def profile_case():
     inf = m.info()
     print(json.dumps({"profile_case": "c2 geometry, nt=30", "nnz": inf["nnz"], "rows": inf["n_rows"],
                       "build_kernel_ms": inf["build_kernel_ms"], "jacobi_sweeps": st["iterations"],
-                      "bytes_per_sweep": st["bytes_per_sweep"], "jacobi_s": st["seconds"]}))
+                      "bytes_per_sweep": st["bytes_per_sweep"],
+                      "stream_bytes_per_sweep": st["stream_bytes_per_sweep"], "pack_ms": st["pack_ms"],
+                      "jacobi_s": st["seconds"]}))
     m.free()
     return 0
 
@@ -414,9 +647,19 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--profile-case", action="store_true", help="small case for ncu captures")
+    ap.add_argument("--batched-only", action="store_true", help="only the batched form (256 uneven MDPs)")
+    ap.add_argument("--no-batched", action="store_true", help="skip the batched form")
+    ap.add_argument("--served-only", action="store_true", help="only the served form (request server)")
+    ap.add_argument("--no-served", action="store_true", help="skip the served form")
     args = ap.parse_args()
     if args.profile_case:
         return profile_case()
+    if args.batched_only:
+        print(json.dumps({"batched": run_batched()}), flush=True)
+        return 0
+    if args.served_only:
+        print(json.dumps({"served": run_served()}), flush=True)
+        return 0
     ws, rank, local = _dist()
     if args.impl == "reference":
         out = run_reference(args, ws, rank, local)
@@ -431,6 +674,10 @@ def main():
         dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=600))
     try:
         line = run_ours(args, ws, rank, local)
+        if rank == 0 and ws == 1 and not args.no_batched:
+            line["batched"] = run_batched()
+        if rank == 0 and ws == 1 and not args.no_served:
+            line["served"] = run_served()
         if rank == 0:
             print(json.dumps(line), flush=True)
     finally:

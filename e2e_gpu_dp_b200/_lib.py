@@ -63,13 +63,45 @@ class ModelInfo(C.Structure):
 
 class ViOpts(C.Structure):
     _fields_ = [("method", C.c_int32), ("threshold", C.c_float), ("max_iter", C.c_int32),
-                ("timeout_s", C.c_double), ("fp64_check", C.c_int32), ("reserved", C.c_int32)]
+                ("timeout_s", C.c_double), ("fp64_check", C.c_int32), ("schedule", C.c_int32)]
 
 
 class ViStats(C.Structure):
     _fields_ = [("iterations", C.c_int32), ("residual", C.c_double), ("seconds", C.c_double),
                 ("fp64_max_abs_err", C.c_double), ("fp64_max_rel_err", C.c_double),
-                ("bytes_per_sweep", C.c_int64)]
+                ("bytes_per_sweep", C.c_int64), ("stream_bytes_per_sweep", C.c_int64),
+                ("pack_ms", C.c_double), ("sweep_seconds", C.c_double)]
+
+
+class BatchStats(C.Structure):
+    _fields_ = [("jobs", C.c_int32), ("launches", C.c_int32), ("groups", C.c_int32),
+                ("tune", C.c_int32), ("grid", C.c_int32), ("graph", C.c_int32),
+                ("seconds", C.c_double), ("pack_ms", C.c_double), ("tune_ms", C.c_double),
+                ("stream_bytes", C.c_int64)]
+
+
+class ServerOpts(C.Structure):
+    _fields_ = [("hbm_budget", C.c_int64), ("max_batch", C.c_int32), ("schedule", C.c_int32)]
+
+
+class Request(C.Structure):
+    _fields_ = [("field_id", C.c_int32), ("num_ac_angles", C.c_int32), ("i_term", C.c_int32),
+                ("j_term", C.c_int32), ("i_start", C.c_int32), ("j_start", C.c_int32),
+                ("keep_outputs", C.c_int32), ("reserved", C.c_int32), ("tag", C.c_int64)]
+
+
+class Result(C.Structure):
+    _fields_ = [("request_id", C.c_int64), ("tag", C.c_int64), ("status", C.c_int32),
+                ("action_at_start", C.c_int32), ("value_at_start", C.c_float), ("batch_size", C.c_int32),
+                ("latency_ms", C.c_double), ("queue_ms", C.c_double)]
+
+
+class ServerStats(C.Structure):
+    _fields_ = [("completed", C.c_int64), ("failed", C.c_int64), ("pending", C.c_int64),
+                ("batches", C.c_int64), ("models_built", C.c_int64), ("models_evicted", C.c_int64),
+                ("models_resident", C.c_int64), ("bytes_in_use", C.c_int64), ("budget_bytes", C.c_int64),
+                ("max_batch", C.c_int32), ("reserved", C.c_int32), ("build_ms", C.c_double),
+                ("solve_ms", C.c_double)]
 
 
 # every exported symbol of include/e2e_dp.h with its signature
@@ -93,6 +125,20 @@ SIGNATURES = {
                                  C.POINTER(ViStats), C.c_void_p]),
     "e2e_spvi_solve_noalloc": (C.c_int, [C.c_void_p, C.POINTER(ViOpts), C.c_void_p, C.c_void_p,
                                          C.POINTER(ViStats), C.c_void_p]),
+    "e2e_spvi_solve_batch": (C.c_int, [C.POINTER(C.c_void_p), C.c_int32, C.POINTER(ViOpts),
+                                       C.POINTER(C.c_void_p), C.POINTER(C.c_void_p),
+                                       C.POINTER(BatchStats), C.c_void_p]),
+    "e2e_build_models": (C.c_int, [C.POINTER(Problem), C.POINTER(Fields), C.c_int32, C.c_int,
+                                   C.POINTER(BuildOpts), C.c_int32, C.POINTER(C.c_void_p)]),
+    "e2e_server_create": (C.c_int, [C.POINTER(ServerOpts), C.POINTER(C.c_void_p)]),
+    "e2e_server_add_field": (C.c_int, [C.c_void_p, C.POINTER(Problem), C.POINTER(Fields), C.c_int,
+                                       C.POINTER(C.c_int32)]),
+    "e2e_server_submit": (C.c_int, [C.c_void_p, C.POINTER(Request), C.POINTER(C.c_int64)]),
+    "e2e_server_poll": (C.c_int, [C.c_void_p, C.POINTER(Result), C.c_int32, C.POINTER(C.c_int32),
+                                  C.c_double]),
+    "e2e_server_fetch": (C.c_int, [C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p, C.c_int]),
+    "e2e_server_get_stats": (C.c_int, [C.c_void_p, C.POINTER(ServerStats)]),
+    "e2e_server_destroy": (C.c_int, [C.c_void_p]),
 }
 
 _lib = None

@@ -98,14 +98,16 @@ class Model:
 
     def solve(self, method: str = "layered", threshold: float = 0.1, max_iter: int = 0,
               timeout_s: float = 0.0, fp64_check: bool = False, value=None, policy=None,
-              stream=None) -> Tuple:
+              stream=None, schedule: int = 0) -> Tuple:
         """Value iteration.  ``method``: "layered" (backward sweep + verification
         sweep) or "jacobi" (reference semantics).  With ``value``/``policy`` CUDA
-        tensors the results stay on the device; otherwise numpy arrays are returned."""
+        tensors the results stay on the device; otherwise numpy arrays are returned.
+        ``schedule``: the ``schedule`` word of e2e_vi_opts (0 = automatic; bits 0-3
+        warps per chunk, bit 8 set: bits 4-6 sweep tuning)."""
         inf = self.info()
         ns = inf["ns"]
         o = _lib.ViOpts(1 if method == "layered" else 0, threshold, max_iter, timeout_s,
-                        1 if fp64_check else 0, 0)
+                        1 if fp64_check else 0, schedule)
         stats = _lib.ViStats()
         if value is not None and hasattr(value, "data_ptr"):
             where = _lib.E2E_DEVICE if _is_device(value) else _lib.E2E_HOST
@@ -132,6 +134,44 @@ class Model:
             pass
 
 
+def solve_batch(models, values, policies, schedule: int = 0, stream=None) -> Dict:
+    """Layered solves of many models in one persistent launch (e2e_spvi_solve_batch).
+    ``values`` / ``policies``: CUDA tensors (float32 / int32), one per model, of
+    its ``ns`` states.  Returns the batch statistics."""
+    n = len(models)
+    hs = (C.c_void_p * n)(*[m.handle for m in models])
+    vs = (C.c_void_p * n)(*[v.data_ptr() for v in values])
+    ps = (C.c_void_p * n)(*[p.data_ptr() for p in policies])
+    o = _lib.ViOpts(1, 0.1, 0, 0.0, 0, schedule)
+    st = _lib.BatchStats()
+    check(lib().e2e_spvi_solve_batch(hs, n, C.byref(o), vs, ps, C.byref(st), _stream_ptr(stream)))
+    return {f: getattr(st, f) for f, _ in _lib.BatchStats._fields_}
+
+
+def build_models(probs, fields_list, count_type: str = "auto", workers: int = 4):
+    """Many builds at once (e2e_build_models): ``workers`` host threads, one
+    stream each.  Fields all on the host or all CUDA tensors."""
+    n = len(probs)
+    keep = []
+    fs = (_lib.Fields * n)()
+    where = None
+    for i, fl in enumerate(fields_list):
+        w, f, k = _fields_ptrs(fl)
+        if where is None:
+            where = w
+        elif w != where:
+            raise ValueError("fields must all be on the host or all on the device")
+        fs[i] = f
+        keep.append(k)
+    ps = (_lib.Problem * n)(*[c_problem(p) for p in probs])
+    o = _lib.BuildOpts(_COUNT[count_type], 0, 0, 0, 0)
+    out = (C.c_void_p * n)()
+    check(lib().e2e_build_models(ps, fs, n, where if where is not None else _lib.E2E_HOST, C.byref(o),
+                                 workers, out))
+    del keep
+    return [Model(out[i], probs[i]) for i in range(n)]
+
+
 def build_model(prob: Problem, fields: Dict, count_type: str = "auto", stream=None) -> Model:
     """Monte-Carlo transition build of every (t, cell, action) row on the GPU."""
     keep = []
@@ -152,3 +192,81 @@ def build_model(prob: Problem, fields: Dict, count_type: str = "auto", stream=No
     check(lib().e2e_build_model(C.byref(cp), C.byref(f), where, C.byref(o), C.byref(h),
                                 _stream_ptr(stream)))
     return Model(h.value, prob)
+
+
+def _fields_ptrs(fields: Dict):
+    """(where, Fields struct, keep-alive list) for host numpy or CUDA tensor fields."""
+    keep = []
+    if all(_is_device(fields[k]) for k in ("u", "v", "Yi", "s", "mask")):
+        where = _lib.E2E_DEVICE
+        ptr = {k: fields[k].data_ptr() for k in fields}
+    else:
+        where = _lib.E2E_HOST
+        ptr = {}
+        for k in ("u", "v", "ui", "vi", "Yi", "s", "mask"):
+            a = np.ascontiguousarray(fields[k], dtype=np.int32 if k == "mask" else np.float32)
+            keep.append(a)
+            ptr[k] = a.ctypes.data
+    f = _lib.Fields(ptr["u"], ptr["v"], ptr["ui"], ptr["vi"], ptr["Yi"], ptr["s"], ptr["mask"])
+    return where, f, keep
+
+
+class Server:
+    """The request server of the C ABI (e2e_server_*): resident fields, cached
+    base models, continuous batching of plan requests on one GPU."""
+
+    def __init__(self, hbm_budget: int = 0, max_batch: int = 0, schedule: int = 0):
+        o = _lib.ServerOpts(hbm_budget, max_batch, schedule)
+        h = C.c_void_p()
+        check(lib().e2e_server_create(C.byref(o), C.byref(h)))
+        self._h = h
+
+    def add_field(self, prob: Problem, fields: Dict) -> int:
+        where, f, keep = _fields_ptrs(fields)
+        cp = c_problem(prob)
+        fid = C.c_int32()
+        check(lib().e2e_server_add_field(self._h, C.byref(cp), C.byref(f), where, C.byref(fid)))
+        del keep
+        return fid.value
+
+    def submit(self, field_id: int, headings: int, target, start, keep_outputs: bool = False,
+               tag: int = 0) -> int:
+        r = _lib.Request(field_id, headings, int(target[0]), int(target[1]), int(start[0]), int(start[1]),
+                         1 if keep_outputs else 0, 0, tag)
+        rid = C.c_int64()
+        check(lib().e2e_server_submit(self._h, C.byref(r), C.byref(rid)))
+        return rid.value
+
+    def poll(self, max_results: int = 1024, wait_s: float = 0.0):
+        buf = (_lib.Result * max_results)()
+        n = C.c_int32()
+        check(lib().e2e_server_poll(self._h, buf, max_results, C.byref(n), wait_s))
+        return [{f: getattr(buf[i], f) for f, _ in _lib.Result._fields_} for i in range(n.value)]
+
+    def fetch(self, request_id: int, ns: int):
+        V = np.empty(ns, np.float32)
+        pi = np.empty(ns, np.int32)
+        check(lib().e2e_server_fetch(self._h, request_id, V.ctypes.data, pi.ctypes.data, _lib.E2E_HOST))
+        return V, pi
+
+    def stats(self) -> Dict:
+        st = _lib.ServerStats()
+        check(lib().e2e_server_get_stats(self._h, C.byref(st)))
+        return {f: getattr(st, f) for f, _ in _lib.ServerStats._fields_}
+
+    def close(self) -> None:
+        if self._h:
+            lib().e2e_server_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

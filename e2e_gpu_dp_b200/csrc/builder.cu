@@ -23,7 +23,10 @@
 //    one atomicAdd per CTA, with the row's tile-relative offset and R = sumR/nrzns;
 //  * K2 scans the tile lengths, K3 moves every tile into canonical CSR order and
 //    writes row_ptr.
+#include <mutex>
+
 #include "common.cuh"
+
 #include "kernels.h"
 
 namespace e2e {
@@ -426,6 +429,7 @@ __global__ void __launch_bounds__(1024) k_build_tiles(BuildArgs A) {
   const int64_t grow = ((int64_t)T * nc + cell) * P.na + a;
   A.row_off[grow] = (uint32_t)excl;
   A.R[grow] = sumR / P.nrzns;  // compute_mean, src/build_model.cu:567
+  if (A.sumR) A.sumR[grow] = sumR;  // kept for re-targeting (served requests)
   if (mode == MODE_LOST) return;
   unsigned long long off = wbase + (unsigned long long)excl;
   if (off + (unsigned long long)nnz > (unsigned long long)A.stage_cap) return;  // host re-runs
@@ -590,9 +594,21 @@ static cudaError_t launch_one(const BuildArgs& A, int n_layers, cudaStream_t st)
   dim3 grid((unsigned)A.tiles_per_layer, (unsigned)n_layers);
   dim3 block((unsigned)(32u << A.lanes_log2));
   size_t sm = build_smem_bytes(A.P.na, A.P.nm, A.rc);
-  cudaError_t e = cudaFuncSetAttribute(k_build_tiles<CntT, UNIT>,
-                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-  if (e != cudaSuccess) return e;
+  {
+    // the shared-memory cap only grows: builds on other host threads may be
+    // launching this kernel with a larger need at the same time
+    static std::mutex mu;
+    static int cap_set[64] = {};
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    std::lock_guard<std::mutex> lk(mu);
+    if (dev >= 0 && dev < 64 && (int)sm > cap_set[dev]) {
+      e = cudaFuncSetAttribute(k_build_tiles<CntT, UNIT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+      if (e != cudaSuccess) return e;
+      cap_set[dev] = (int)sm;
+    }
+  }
   k_build_tiles<CntT, UNIT><<<grid, block, sm, st>>>(A);
   return cudaGetLastError();
 }

@@ -324,10 +324,17 @@ ViModel vi_model(const e2e_model* m) {
 
 void free_model_buffers(e2e_model* m) {
   // pool memory, released in stream order on the legacy default stream
+  if (m->pack) {
+    free_pack(m->pack);
+    delete m->pack;
+    m->pack = nullptr;
+  }
   if (m->row_ptr) cudaFreeAsync(m->row_ptr, 0);
   if (m->col) cudaFreeAsync(m->col, 0);
   if (m->cnt) cudaFreeAsync(m->cnt, 0);
   if (m->R) cudaFreeAsync(m->R, 0);
+  if (m->sumR) cudaFreeAsync(m->sumR, 0);
+  m->sumR = nullptr;
   m->row_ptr = nullptr;
   m->col = nullptr;
   m->cnt = nullptr;
@@ -388,6 +395,7 @@ extern "C" e2e_status e2e_build_model(const e2e_problem* p, const e2e_fields* f,
   BuildPlan plan;
   e2e_status s = plan_build(p, count_bits, o.stage_hint, &plan);
   if (s != E2E_OK) return s;
+  plan.keep_sums = o.keep_reward_parts != 0;
 
   DeviceScratch scratch(st);
   FieldsOnDevice fd;
@@ -475,6 +483,10 @@ e2e_status run_build(const e2e_problem* p, const DevFields& F, const BuildPlan& 
   // model R (state-major, last layer zero as src/build_model.cu:1173-1176)
   CK(dalloc((void**)&m->R, sizeof(float) * (size_t)pl.ns * pl.na, st));
   CK(cudaMemsetAsync(m->R, 0, sizeof(float) * (size_t)pl.ns * pl.na, st));
+  if (pl.keep_sums) {
+    CK(dalloc((void**)&m->sumR, sizeof(float) * (size_t)pl.ns * pl.na, st));
+    CK(cudaMemsetAsync(m->sumR, 0, sizeof(float) * (size_t)pl.ns * pl.na, st));
+  }
   uint32_t* row_off = nullptr;
   int64_t* tile_base = nullptr;
   int32_t* tile_len = nullptr;
@@ -522,6 +534,7 @@ e2e_status run_build(const e2e_problem* p, const DevFields& F, const BuildPlan& 
     A.tile_base = tile_base;
     A.tile_len = tile_len;
     A.R = m->R;
+    A.sumR = m->sumR;
     A.pool = pool;
     A.pool_units = pool_units;
     CK(cudaEventRecord(ev[0], st));
@@ -683,19 +696,16 @@ extern "C" e2e_status e2e_model_copy_to_host(const e2e_model* m, int64_t* row_pt
 // ---------------------------------------------------------------------------------
 namespace e2e {
 
-e2e_status solve_on_device(const e2e_model* m, const e2e_vi_opts& o, float* dV, int32_t* dpi,
-                           e2e_vi_stats* stats, cudaStream_t st) {
+// The sliced copy of the model that the sweeps stream (built once per model).
+e2e_status ensure_pack(const e2e_model* m, double* pack_ms, cudaStream_t st) {
+  *pack_ms = 0.0;
+  if (m->pack) return E2E_OK;
   const ViModel M = vi_model(m);
-  const int64_t ns = m->ns;
-  DeviceScratch scratch(st);
-  float* W = nullptr;
-  unsigned long long* resid = nullptr;
-  const int max_iter = o.max_iter > 0 ? o.max_iter : (m->nt > 0 ? m->nt + 2 : 100000);
-  CK(dalloc((void**)&W, sizeof(float) * (size_t)ns, st));
-  scratch.add(W);
-  CK(dalloc((void**)&resid, sizeof(unsigned long long) * (size_t)(max_iter + 2), st));
-  scratch.add(resid);
-  CK(cudaMemsetAsync(resid, 0, sizeof(unsigned long long) * (size_t)(max_iter + 2), st));
+  const bool geo = m->layered && m->has_prob && m->ncells > 0 &&
+                   (int64_t)m->prob.gsize * m->prob.gsize == m->ncells;
+  const int g = geo ? m->prob.gsize : 0;
+  const int del = geo ? (m->prob.neighb_gsize - 1) / 2 : 0;
+  const int64_t nc = m->layered ? m->ncells : 0;
   cudaEvent_t e0, e1;
   CK(cudaEventCreate(&e0));
   CK(cudaEventCreate(&e1));
@@ -703,26 +713,80 @@ e2e_status solve_on_device(const e2e_model* m, const e2e_vi_opts& o, float* dV, 
     cudaEvent_t a, b;
     ~EvGuard() { cudaEventDestroy(a); cudaEventDestroy(b); }
   } evg{e0, e1};
+  auto* ps = new PackStore();
+  CK(cudaEventRecord(e0, st));
+  cudaError_t e = build_pack(M, nc, g, del, ps, st);
+  if (e != cudaSuccess) {
+    free_pack(ps);
+    delete ps;
+    return cuda_fail(e, "build_pack");
+  }
+  CK(cudaEventRecord(e1, st));
+  CK(cudaEventSynchronize(e1));
+  float ms = 0.f;
+  CK(cudaEventElapsedTime(&ms, e0, e1));
+  *pack_ms = ms;
+  m->pack = ps;
+  return E2E_OK;
+}
+
+e2e_status solve_on_device(const e2e_model* m, const e2e_vi_opts& o, float* dV, int32_t* dpi,
+                           e2e_vi_stats* stats, cudaStream_t st) {
+  const int64_t ns = m->ns;
+  const int gsel = o.schedule & 15;
+  if ((o.schedule & ~0x17f) || (gsel != 0 && gsel != 1 && gsel != 2 && gsel != 4 && gsel != 8))
+    return fail(E2E_ERR_INVALID,
+                "schedule: bits 0-3 warps per chunk (0, 1, 2, 4, 8), bits 4-6 sweep tuning, bit 8 tuning given");
+  // sweep tuning: given, or the defaults measured on B200 (layered: look-ahead
+  // kernel, next layer's chunks prefetched into L2; Jacobi: lean kernel)
+  const bool tune_given = (o.schedule & 0x100) != 0;
+  const int tune_layered = tune_given ? (o.schedule >> 4) & 7 : VI_TUNE_PF_NEXT;
+  const int tune_jacobi = tune_given ? (o.schedule >> 4) & 7 : VI_TUNE_LEAN;
+  double pack_ms = 0.0;
+  {
+    e2e_status ps = ensure_pack(m, &pack_ms, st);
+    if (ps != E2E_OK) return ps;
+  }
+  const ViPack& P = m->pack->v;
+  DeviceScratch scratch(st);
+  float* W = nullptr;
+  unsigned long long* resid = nullptr;
+  const int max_iter = o.max_iter > 0 ? o.max_iter : (m->nt > 0 ? m->nt + 2 : 100000);
+  CK(dalloc((void**)&W, sizeof(float) * (size_t)ns, st));
+  scratch.add(W);
+  CK(dalloc((void**)&resid, sizeof(unsigned long long) * (size_t)(max_iter + 3), st));
+  scratch.add(resid);
+  CK(cudaMemsetAsync(resid, 0, sizeof(unsigned long long) * (size_t)(max_iter + 3), st));
+  // last slot: barrier count and error bits of the persistent layered sweep
+  unsigned int* syncw = reinterpret_cast<unsigned int*>(resid + max_iter + 2);
+  cudaEvent_t e0, e1, e2;
+  CK(cudaEventCreate(&e0));
+  CK(cudaEventCreate(&e1));
+  CK(cudaEventCreate(&e2));
+  struct EvGuard {
+    cudaEvent_t a, b, c;
+    ~EvGuard() { cudaEventDestroy(a); cudaEventDestroy(b); cudaEventDestroy(c); }
+  } evg{e0, e1, e2};
   auto t_start = std::chrono::steady_clock::now();
   int iters = 0;
   double last_res = 0.0;
+  bool layered_pass = false;
   const int64_t pbytes = m->index_bits == 32 ? 4 : 8;
   const int64_t cbytes = m->count_type == E2E_COUNT_U16 ? 2 : 4;
   int64_t sweep_bytes = (m->n_rows + 1) * pbytes + m->nnz * (4 + cbytes) + ns * m->na * 4 + ns * 12;
   CK(cudaEventRecord(e0, st));
   if (o.method == 1) {
-    if (!m->layered || m->ncells <= 0 || m->nt <= 0)
+    if (!m->layered || m->ncells <= 0 || m->nt <= 0 || P.nlayers < 2)
       return fail(E2E_ERR_UNSUPPORTED, "layered solve needs a time-layered model (nt, ncells known)");
-    const int64_t nc = m->ncells;
-    // last layer (no rows): V = max_a R
-    CK(launch_vi_sweep(M, m->n_row_states, ns, dV, dV, dpi, nullptr, st));
-    for (int64_t t = (m->n_row_states / nc) - 1; t >= 0; --t)
-      CK(launch_vi_sweep(M, t * nc, (t + 1) * nc, dV, dV, dpi, nullptr, st));
+    // all layers, last first, in one cooperative launch
+    CK(launch_vi_layered(P, dV, dpi, syncw, gsel, st, tune_layered));
+    CK(cudaEventRecord(e2, st));
+    layered_pass = true;
     // verification sweep (Jacobi from the fixed point): residual must be 0
     int32_t* pi2 = nullptr;
     CK(dalloc((void**)&pi2, sizeof(int32_t) * (size_t)ns, st));
     scratch.add(pi2);
-    CK(launch_vi_sweep(M, 0, ns, dV, W, pi2, resid, st));
+    CK(launch_vi_chunks(P, 0, P.nchunks, dV, W, pi2, resid, st, tune_jacobi));
     unsigned long long h = 0;
     CK(cudaMemcpyAsync(&h, resid, sizeof(h), cudaMemcpyDeviceToHost, st));
     CK(cudaEventRecord(e1, st));
@@ -737,7 +801,7 @@ e2e_status solve_on_device(const e2e_model* m, const e2e_vi_opts& o, float* dV, 
     while (!done) {
       if (iters >= max_iter) break;
       ++iters;
-      CK(launch_vi_sweep(M, 0, ns, a, b, dpi, resid + iters, st));
+      CK(launch_vi_chunks(P, 0, P.nchunks, a, b, dpi, resid + iters, st, tune_jacobi));
       unsigned long long h = 0;
       CK(cudaMemcpyAsync(&h, resid + iters, sizeof(h), cudaMemcpyDeviceToHost, st));
       CK(cudaStreamSynchronize(st));
@@ -765,18 +829,29 @@ e2e_status solve_on_device(const e2e_model* m, const e2e_vi_opts& o, float* dV, 
       return fail(E2E_ERR_NOT_CONVERGED, "max_iter reached before the threshold");
     }
   }
-  float ms = 0.f;
+  {
+    unsigned int herr = 0;
+    CK(cudaMemcpyAsync(&herr, syncw + 1, sizeof(herr), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    if (herr) return fail(E2E_ERR_DEVICE, "a bounded grid barrier of the layered sweep gave up");
+  }
+  float ms = 0.f, ms_pass = 0.f;
   CK(cudaEventElapsedTime(&ms, e0, e1));
+  if (layered_pass) CK(cudaEventElapsedTime(&ms_pass, e0, e2));
   if (stats) {
     stats->iterations = iters;
     stats->residual = last_res;
     stats->seconds = ms * 1e-3;
     stats->bytes_per_sweep = sweep_bytes;
+    stats->stream_bytes_per_sweep = pack_sweep_bytes(P);
+    stats->pack_ms = pack_ms;
+    stats->sweep_seconds = ms_pass * 1e-3;
     stats->fp64_max_abs_err = 0;
     stats->fp64_max_rel_err = 0;
   }
   if (o.fp64_check) {
     if (!m->layered) return fail(E2E_ERR_UNSUPPORTED, "fp64 check needs a time-layered model");
+    const ViModel M = vi_model(m);
     double* Vd = nullptr;
     unsigned long long* err = nullptr;
     CK(dalloc((void**)&Vd, sizeof(double) * (size_t)ns, st));

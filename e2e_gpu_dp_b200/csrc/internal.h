@@ -22,12 +22,15 @@ struct e2e_model {
   int32_t* col = nullptr;    // device
   void* cnt = nullptr;       // device
   float* R = nullptr;        // device, ns * na (state-major)
+  float* sumR = nullptr;     // device, ns * na: reward sums (keep_reward_parts), or null
   uint64_t dropped = 0, misbinned = 0, overflow_rows = 0;
   double build_kernel_ms = 0, assemble_ms = 0;
   int32_t build_launches = 0;
   bool layered = false;      // every transition of a layer-t state leads into layer t+1
   e2e_problem prob{};
   bool has_prob = false;
+  // sliced copy for value iteration, built by the first solve that needs it
+  mutable e2e::PackStore* pack = nullptr;
 };
 
 namespace e2e {
@@ -58,6 +61,7 @@ struct BuildPlan {
   int64_t etiles_per_layer = 0, cells_per_tile = 32;  // emission tiles (one per builder warp)
   int na = 0, rc = 128;
   int64_t stage_cap = 0, pool_units = 0;
+  bool keep_sums = false;  // keep per-row reward sums (e2e_build_opts.keep_reward_parts)
 };
 
 struct FieldsOnDevice {
@@ -80,5 +84,25 @@ void free_model_buffers(e2e_model* m);
 int64_t model_bytes(const e2e_model* m);
 e2e_status solve_on_device(const e2e_model* m, const e2e_vi_opts& o, float* dV, int32_t* dpi,
                            e2e_vi_stats* stats, cudaStream_t st);
+// build the model's sliced copy for the sweeps if it has none yet
+e2e_status ensure_pack(const e2e_model* m, double* pack_ms, cudaStream_t st);
+
+// One layered solve of a batch: a model, its outputs and, for a served
+// request, the re-targeted R around its target (ViJob fields).
+struct BatchJobSpec {
+  const e2e_model* m = nullptr;
+  float* V = nullptr;
+  int32_t* pi = nullptr;
+  const float* Rwin = nullptr;
+  int ti = 0, tj = 0, tsg = 0, wi0 = 0, wj0 = 0, wh = 0, ww = 0;
+};
+struct BatchResult {
+  int launches = 0, groups = 0, tune = 0, grid = 0, graph = 0;
+  double seconds = 0, pack_ms = 0, tune_ms = 0;
+  int64_t stream_bytes = 0;
+};
+// schedule: e2e_vi_opts.schedule (bit 9: direct launch instead of a CUDA graph)
+e2e_status solve_batch(const std::vector<BatchJobSpec>& jobs, int schedule, cudaStream_t st,
+                       BatchResult* res);
 
 }  // namespace e2e

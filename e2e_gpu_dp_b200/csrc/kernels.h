@@ -36,6 +36,7 @@ struct BuildArgs {
   int64_t* tile_base;            // per tile: staging offset
   int32_t* tile_len;             // per tile: entries
   float* R;                      // per row (state-major, Ns * na)
+  float* sumR;                   // nullable: per-row reward sums (before the division)
   uint32_t* pool;                // pool_units x m*m dense histograms
   int64_t pool_units;
 };
@@ -87,5 +88,82 @@ cudaError_t launch_vi_sweep_f64(const ViModel& M, int64_t s_begin, int64_t s_end
 // max |V - Vd| into err[0], max |Vd| into err[1] (bits of non-negative doubles)
 cudaError_t launch_compare_f64(const float* V, const double* Vd, int64_t n,
                                unsigned long long* err, cudaStream_t st);
+
+// ---- sliced copy of a model for value iteration (vi_pack.cu) ------------------
+// entry layouts of the sliced copy
+enum : int {
+  ENT_PACKED = 0,  // uint32 per entry: 16-bit window offset | uint16 count << 16
+  ENT_OFF16 = 1,   // uint16 window offset + uint32 count / float value arrays
+  ENT_I32 = 2      // int32 column + count array (models without window geometry)
+};
+
+struct ViPack {
+  int64_t ns, nc;          // states; states per layer (ns when the model has no layers)
+  int64_t cpl, nchunks;    // chunks of 32 states per layer; all chunks
+  int64_t n_row_states;    // states that own rows
+  int64_t slot_rows;       // slot rows of 32 entries
+  int nlayers, na, na_pad, nrzns, count_type, ent_mode;
+  int g, del;              // grid side and window half-width (window-offset column base)
+  const int64_t* chunk_slot;  // nchunks + 1: first slot row of each chunk
+  const uint16_t* maxlen;     // nchunks * na_pad: slot rows per (chunk, action)
+  const void* col;            // slot_rows * 32: packed entries, uint16 offsets or int32 columns
+  const void* cnt;            // slot_rows * 32: counts / values (null for ENT_PACKED)
+  const float* R;             // nchunks * na * 32: [chunk][action][lane]
+};
+
+struct PackStore {
+  ViPack v{};
+  void* bufs[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
+  int64_t bytes = 0;
+};
+
+// Build the sliced copy of a state-major CSR model.  nc = states per layer
+// (0: none); g, del = grid side and window half-width of a layered model built
+// on a g x g grid (0: unknown, int32 columns).
+cudaError_t build_pack(const ViModel& M, int64_t nc, int g, int del, PackStore* out, cudaStream_t st);
+void free_pack(PackStore* p);
+// bytes one sweep over the pack moves (entries with padding, R, tables, V)
+int64_t pack_sweep_bytes(const ViPack& P);
+// tune bits of the sweeps: L2 bulk prefetch of the chunk a warp takes next
+// (the next layer's, when layered) and/or of the chunk it starts; the lean
+// kernel (no entry look-ahead, 8 CTAs per SM) instead of the look-ahead one
+enum : int { VI_TUNE_PF_NEXT = 1, VI_TUNE_PF_CURRENT = 2, VI_TUNE_LEAN = 4 };
+// One Jacobi sweep over chunks [c_begin, c_end).
+cudaError_t launch_vi_chunks(const ViPack& P, int64_t c_begin, int64_t c_end, const float* Vin,
+                             float* Vout, int32_t* pi, unsigned long long* resid, cudaStream_t st,
+                             int tune);
+// The whole layered schedule in one cooperative launch, in place on V.
+// sync: two zeroed words (barrier count, error bits); groups: warps per chunk
+// (1, 2, 4, 8; 0 picks one).
+cudaError_t launch_vi_layered(const ViPack& P, float* V, int32_t* pi, unsigned int* sync, int groups,
+                              cudaStream_t st, int tune);
+
+
+// ---- many models in one persistent launch (batched and served solves) ----------
+// A job is one model's layered solve: V and policy outputs, and optionally a
+// re-targeted copy of R for the cells around a target (served requests).
+struct ViJob {
+  ViPack P;
+  float* V;
+  int32_t* pi;
+  const float* Rwin;     // null, or R of cells [wi0, wi0+wh) x [wj0, wj0+ww):
+                         // [layer < nlayers-1][wh][ww][na]
+  int ti, tj, tsg;       // terminal subgrid of the target (when Rwin is set)
+  int wi0, wj0, wh, ww;
+};
+struct ViBatchHeader {
+  int njobs, max_layers, pad0, pad1;
+};
+// Device table: header | jobs[job_cap] | cum[job_cap + 1] | nact[layer_cap].
+// Jobs sorted by nlayers, descending; cum = prefix sums of their chunks per
+// layer; nact[k] = jobs with more than k layers.  Step k of the launch works
+// on layer nlayers-1-k of jobs [0, nact[k]): chunk items [0, cum[nact[k]]).
+size_t vi_batch_table_bytes(int job_cap, int layer_cap);
+constexpr size_t kViBatchJobsOffset = 64;  // header padded to 64 bytes
+// CTAs of the batch kernel that fit on the device at once
+int vi_batch_capacity(int ent_mode, int count_type, int tune);
+// sync: two zeroed words; grid <= vi_batch_capacity (co-resident CTAs)
+cudaError_t launch_vi_batch(const void* table, int job_cap, int ent_mode, int count_type, int groups,
+                            int grid, int tune, unsigned int* sync, cudaStream_t st);
 
 }  // namespace e2e

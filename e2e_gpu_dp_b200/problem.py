@@ -247,16 +247,10 @@ def _fourier_mode(rng: np.random.Generator, X: np.ndarray, Y: np.ndarray, L: flo
     return acc / (m if m > 0 else 1.0)
 
 
-def make_fields(prob: Problem, spec: FieldSpec) -> Dict[str, np.ndarray]:
-    """Seeded fields in the reference layout (see the module docstring).
-
-    Mean flow: ``u = -A sin(pi x/L) cos(pi y/L)``, ``v = A cos(pi x/L) sin(pi y/L)``
-    with ``L = g*dx`` at cell centres, time invariant.  Modes: per k, an
-    independent low-frequency Fourier field for ui and for vi, normalised to
-    unit max, time invariant.  Coefficients ``Y[t, rzn, k] ~ N(0, sigma_k)``
-    independent over (t, rzn, k).  Obstacles: i.i.d. cells with probability
-    ``obstacle_frac``, constant over t, never on the terminal subgrid.
-    """
+def field_parts(prob: Problem, spec: FieldSpec) -> Dict[str, np.ndarray]:
+    """The time-invariant pieces of the seeded fields: u2, v2, s2 (g, g),
+    ui1, vi1 (nm, g, g), obs (g, g), and Yi (nt, nrzns, nm).  ``make_fields``
+    repeats them over t; a device copy can do the same without host copies."""
     prob.validate()
     g, nt, nm, nr = prob.gsize, prob.nt, prob.nmodes, prob.nrzns
     ss = np.random.SeedSequence(spec.seed)
@@ -267,23 +261,41 @@ def make_fields(prob: Problem, spec: FieldSpec) -> Dict[str, np.ndarray]:
     L = g * prob.dx
     u2 = -spec.A * np.sin(math.pi * X / L) * np.cos(math.pi * Yc / L)
     v2 = spec.A * np.cos(math.pi * X / L) * np.sin(math.pi * Yc / L)
-    u = np.ascontiguousarray(np.broadcast_to(u2.astype(np.float32), (nt, g, g)))
-    v = np.ascontiguousarray(np.broadcast_to(v2.astype(np.float32), (nt, g, g)))
     ui1 = np.stack([_fourier_mode(r_modes, X, Yc, L) for _ in range(nm)]).astype(np.float32)
     vi1 = np.stack([_fourier_mode(r_modes, X, Yc, L) for _ in range(nm)]).astype(np.float32)
-    ui = np.ascontiguousarray(np.broadcast_to(ui1, (nt, nm, g, g)))
-    vi = np.ascontiguousarray(np.broadcast_to(vi1, (nt, nm, g, g)))
     sig = np.array([spec.sigma0 / (spec.sigma_base ** k) for k in range(nm)], dtype=np.float64)
     Yi = (r_y.standard_normal((nt, nr, nm)) * sig[None, None, :]).astype(np.float32)
     s2 = np.full((g, g), spec.scalar, dtype=np.float64)
     if spec.scalar_wave:
         s2 = s2 + spec.scalar_wave * _fourier_mode(r_s, X, Yc, L)
-    s = np.ascontiguousarray(np.broadcast_to(s2.astype(np.float32), (nt, g, g)))
     obs = (r_obs.random((g, g)) < spec.obstacle_frac).astype(np.int32)
     ts = prob.term_subgrid_size
     obs[prob.i_term:prob.i_term + ts, prob.j_term:prob.j_term + ts] = 0
-    mask = np.ascontiguousarray(np.broadcast_to(obs, (nt, g, g))).astype(np.int32)
-    return {"u": u, "v": v, "ui": ui, "vi": vi, "Yi": Yi, "s": s, "mask": mask}
+    return {"u2": u2.astype(np.float32), "v2": v2.astype(np.float32), "ui1": ui1, "vi1": vi1,
+            "Yi": Yi, "s2": s2.astype(np.float32), "obs": obs}
+
+
+def expand_parts(prob: Problem, parts: Dict[str, np.ndarray], broadcast) -> Dict:
+    """Repeat the time-invariant parts over t with ``broadcast(array, shape)``."""
+    g, nt, nm = prob.gsize, prob.nt, prob.nmodes
+    return {"u": broadcast(parts["u2"], (nt, g, g)), "v": broadcast(parts["v2"], (nt, g, g)),
+            "ui": broadcast(parts["ui1"], (nt, nm, g, g)), "vi": broadcast(parts["vi1"], (nt, nm, g, g)),
+            "Yi": parts["Yi"], "s": broadcast(parts["s2"], (nt, g, g)),
+            "mask": broadcast(parts["obs"], (nt, g, g))}
+
+
+def make_fields(prob: Problem, spec: FieldSpec) -> Dict[str, np.ndarray]:
+    """Seeded fields in the reference layout (see the module docstring).
+
+    Mean flow: ``u = -A sin(pi x/L) cos(pi y/L)``, ``v = A cos(pi x/L) sin(pi y/L)``
+    with ``L = g*dx`` at cell centres, time invariant.  Modes: per k, an
+    independent low-frequency Fourier field for ui and for vi, normalised to
+    unit max, time invariant.  Coefficients ``Y[t, rzn, k] ~ N(0, sigma_k)``
+    independent over (t, rzn, k).  Obstacles: i.i.d. cells with probability
+    ``obstacle_frac``, constant over t, never on the terminal subgrid.
+    """
+    parts = field_parts(prob, spec)
+    return expand_parts(prob, parts, lambda a, shape: np.ascontiguousarray(np.broadcast_to(a, shape)))
 
 
 def write_reference_inputs(dirpath: str, fields: Dict[str, np.ndarray]) -> None:

@@ -31,7 +31,7 @@
 extern "C" {
 #endif
 
-#define E2E_DP_ABI_VERSION 1
+#define E2E_DP_ABI_VERSION 2
 
 typedef enum {
   E2E_OK = 0,
@@ -104,7 +104,8 @@ typedef struct {
   int32_t count_type;   /* E2E_COUNT_AUTO (u16 when nrzns < 65536), E2E_COUNT_U16 or _U32 */
   int32_t tile_cells;   /* 0 = default (32); cells per builder tile, multiple of 32 */
   int64_t stage_hint;   /* 0 = default; initial staging capacity in entries */
-  int32_t keep_reward_parts; /* 1: also keep per-entry reward sums for target re-use (server) */
+  int32_t keep_reward_parts; /* 1: also keep each row's reward sum (before the division by nrzns),
+                                which re-targeting a model needs (the request server) */
   int32_t reserved;
 } e2e_build_opts;
 
@@ -139,7 +140,10 @@ typedef struct {
   int32_t max_iter;      /* 0 = nt + 2 */
   double timeout_s;      /* host wall-clock limit, 0 = none */
   int32_t fp64_check;    /* 1: FP64 backward solve on the device, report the error of the FP32 values */
-  int32_t reserved;
+  int32_t schedule;      /* 0 = automatic.  Bits 0-3: warps sharing a 32-state chunk in the layered
+                            sweep (0 = auto, 1, 2, 4, 8).  Bit 8 set: bits 4-6 give the sweep
+                            tuning (4: L2 prefetch of the chunk a warp takes next, 5: of the chunk
+                            it starts, 6: lean kernel without entry look-ahead). */
 } e2e_vi_opts;
 
 typedef struct {
@@ -148,7 +152,10 @@ typedef struct {
   double seconds;          /* device time of the solve (CUDA events) */
   double fp64_max_abs_err; /* fp64_check: max |V32 - V64| */
   double fp64_max_rel_err; /* fp64_check: max |V32 - V64| / max |V64| */
-  int64_t bytes_per_sweep; /* algorithmic bytes of one sweep */
+  int64_t bytes_per_sweep; /* algorithmic bytes of one sweep (CSR form: row_ptr, col, count, R, V) */
+  int64_t stream_bytes_per_sweep; /* bytes a sweep over the sliced copy moves (padding included) */
+  double pack_ms;          /* device time spent building the sliced copy in this call (0 if cached) */
+  double sweep_seconds;    /* layered: device time of the backward pass alone */
 } e2e_vi_stats;
 
 /* ---- library ------------------------------------------------------------ */
@@ -207,6 +214,100 @@ e2e_status e2e_model_read_npy(const char* dir, e2e_model** out, void* stream);
 e2e_status e2e_spvi_solve(const e2e_model* m, const e2e_vi_opts* opts /* may be NULL */,
                           int32_t* policy_out, float* value_out, int out_where,
                           e2e_vi_stats* stats /* may be NULL */, void* stream);
+
+/* ---- many layered solves in one launch ---------------------------------------
+ * No counterpart in the reference, which solves one model per spvi_2 process.
+ * Solves n time-layered models with the layered schedule in one persistent
+ * cooperative launch (a grid barrier per layer step, models aligned on their
+ * last layer), captured in a CUDA graph that later batches of the same launch
+ * shape replay.  Results are bit-identical to e2e_spvi_solve(method = 1) on each
+ * model.  value_dev[i] / policy_dev[i]: device buffers of model i's ns states.
+ * opts->schedule as for e2e_spvi_solve, plus bit 9: launch directly, no graph;
+ * without bit 8 the schedule is autotuned on the first batch of each shape.
+ * Calls are serialised inside the library. */
+/* Builds n problems (problems[i] with fields[i], all in fields_where memory)
+ * with e2e_build_model on `workers` host threads, each with its own stream
+ * (0 = 4), so that small builds overlap on the device.  The models are the same
+ * as one build at a time.  On failure every model is freed and out[] is NULL. */
+e2e_status e2e_build_models(const e2e_problem* problems, const e2e_fields* fields, int32_t n,
+                            int fields_where, const e2e_build_opts* opts /* may be NULL */,
+                            int32_t workers, e2e_model** out);
+
+typedef struct {
+  int32_t jobs, launches;
+  int32_t groups, tune, grid; /* schedule used: warps per chunk, tuning bits, CTAs */
+  int32_t graph;              /* 1: replayed from a CUDA graph */
+  double seconds;             /* device time of the launches (CUDA events) */
+  double pack_ms;             /* sliced copies built by this call */
+  double tune_ms;             /* autotuning spent in this call */
+  int64_t stream_bytes;       /* bytes one pass over all the models' sliced copies moves */
+} e2e_batch_stats;
+
+e2e_status e2e_spvi_solve_batch(const e2e_model* const* models, int32_t n, const e2e_vi_opts* opts,
+                                float* const* value_dev, int32_t* const* policy_dev,
+                                e2e_batch_stats* stats /* may be NULL */, void* stream);
+
+/* ---- request server (served form) ---------------------------------------------
+ * No counterpart in the reference, which plans one problem per build_model +
+ * spvi_2 run.  A server keeps velocity fields resident, builds one base model per
+ * (field, heading set) on first use (no terminal cells, reward sums kept), and
+ * answers plan requests by re-targeting R around each request's target and
+ * solving all queued requests in one batched launch (continuous batching).  A
+ * worker thread owns the device work; admission is by an HBM budget, evicting
+ * idle models least recently used.  For integer-valued rewards (the "time"
+ * reward with integer dt, r_outbound, r_terminal) results are bit-identical to
+ * building the model with the request's target and calling e2e_spvi_solve;
+ * otherwise they differ by the rounding of the reward sums.  The terminal
+ * subgrid of a request is its target cell (term_subgrid_size 1). */
+typedef struct e2e_server e2e_server;
+
+typedef struct {
+  int64_t hbm_budget;  /* bytes for models and requests; 0 = 80% of the free memory at creation */
+  int32_t max_batch;   /* requests per launch; 0 = 256 (at most 1024) */
+  int32_t schedule;    /* e2e_vi_opts.schedule of the batched launches (0 = autotuned) */
+} e2e_server_opts;
+
+typedef struct {
+  int32_t field_id;      /* from e2e_server_add_field */
+  int32_t num_ac_angles; /* heading set: this many headings j*2pi/n (speeds as the field's problem) */
+  int32_t i_term, j_term; /* target cell */
+  int32_t i_start, j_start; /* start cell (layer 0): its value and action are returned */
+  int32_t keep_outputs;  /* 1: keep the full value and policy arrays for e2e_server_fetch */
+  int32_t reserved;
+  int64_t tag;           /* returned with the result */
+} e2e_request;
+
+typedef struct {
+  int64_t request_id, tag;
+  int32_t status;        /* E2E_OK or the failure */
+  int32_t action_at_start;
+  float value_at_start;
+  int32_t batch_size;    /* requests solved in the same launch */
+  double latency_ms;     /* submission to completion (host steady clock) */
+  double queue_ms;       /* submission to being taken into a batch */
+} e2e_result;
+
+typedef struct {
+  int64_t completed, failed, pending, batches;
+  int64_t models_built, models_evicted, models_resident;
+  int64_t bytes_in_use, budget_bytes;
+  int32_t max_batch, reserved;
+  double build_ms, solve_ms; /* host time building base models; device time of the batched launches */
+} e2e_server_stats;
+
+e2e_status e2e_server_create(const e2e_server_opts* opts /* may be NULL */, e2e_server** out);
+/* p: grid, nt, nrzns, nmodes, speeds, dt, dx, dy, rewards of the field (its
+ * target and heading count are ignored); fields as for e2e_build_model, copied. */
+e2e_status e2e_server_add_field(e2e_server* s, const e2e_problem* p, const e2e_fields* f, int fields_where,
+                                int32_t* field_id);
+e2e_status e2e_server_submit(e2e_server* s, const e2e_request* r, int64_t* request_id);
+/* up to max finished results; waits up to wait_s seconds when none is ready */
+e2e_status e2e_server_poll(e2e_server* s, e2e_result* out, int32_t max, int32_t* n_out, double wait_s);
+/* full value / policy (ns = nt * gsize^2 each) of a finished keep_outputs request */
+e2e_status e2e_server_fetch(e2e_server* s, int64_t request_id, float* value_out, int32_t* policy_out,
+                            int out_where);
+e2e_status e2e_server_get_stats(e2e_server* s, e2e_server_stats* out);
+e2e_status e2e_server_destroy(e2e_server* s);
 
 /* ---- solve without device allocation ----------------------------------------
  * No counterpart in the reference.  For callers that cannot allocate device

@@ -209,3 +209,42 @@ def test_invalid_problems_are_rejected():
     with pytest.raises(E2EError) as ei:
         api.build_model(many, fields)
     assert ei.value.status == 7
+
+
+@pytest.mark.parametrize("name", ["t_time", "t_custom"])
+def test_every_sweep_schedule_gives_identical_results(built, name):
+    """Sweep schedules (warps per chunk, prefetch, kernel variant) change only
+    the work split; every state's value is the same FMA chain, so results are
+    bit-identical to the default schedule."""
+    torch = pytest.importorskip("torch")
+    prob, fields, model, h, orc = built(name)
+    # reference: Jacobi from V = 0 reads nothing the caller's buffers held
+    Vd, pid, _ = model.solve(method="jacobi", threshold=1e-30, max_iter=prob.nt + 3)
+    for groups in (0, 1, 2, 4, 8):
+        for tune in range(8):
+            # outputs start as NaN: the in-place layered sweep must never read them unwritten
+            V = torch.full((prob.ns,), float("nan"), device="cuda")
+            pi = torch.full((prob.ns,), -7, dtype=torch.int32, device="cuda")
+            _, _, st = model.solve(method="layered", schedule=groups | (tune << 4) | 0x100, value=V, policy=pi)
+            torch.cuda.synchronize()
+            assert st["residual"] == 0.0
+            assert np.array_equal(V.cpu().numpy(), Vd) and np.array_equal(pi.cpu().numpy(), pid), (groups, tune)
+    for tune in range(8):
+        V, pi, _ = model.solve(method="jacobi", threshold=1e-30, max_iter=prob.nt + 3,
+                               schedule=(tune << 4) | 0x100)
+        assert np.array_equal(V, Vd) and np.array_equal(pi, pid), tune
+    with pytest.raises(E2EError):
+        model.solve(method="layered", schedule=3)
+
+
+def test_count_widths_and_layouts_agree(built):
+    """uint32 counts take the separate offset/count layout; the values are the
+    same as the packed uint16 layout's."""
+    prob, fields, model, h, orc = built("t_time")
+    m32 = api.build_model(prob, fields, count_type="u32")
+    assert m32.info()["count_type"] != model.info()["count_type"]
+    for method in ("layered", "jacobi"):
+        V16, pi16, _ = model.solve(method=method, threshold=1e-30, max_iter=prob.nt + 3)
+        V32, pi32, _ = m32.solve(method=method, threshold=1e-30, max_iter=prob.nt + 3)
+        assert np.array_equal(V16, V32) and np.array_equal(pi16, pi32)
+    m32.free()

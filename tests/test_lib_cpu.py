@@ -25,7 +25,7 @@ def test_library_exports_every_declared_symbol():
     for n in names:
         assert hasattr(L, n), n
         assert n in _lib.SIGNATURES, n
-    assert L.e2e_abi_version() == 1
+    assert L.e2e_abi_version() == 2
 
 
 def test_status_strings():
