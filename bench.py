@@ -376,9 +376,10 @@ def run_batched(n_models: int = 256, seed: int = 2024) -> dict:
     seq_s = max(a.elapsed_time(b) / 1e3, time.perf_counter() - t0)
     ref = [(V.clone(), pi.clone()) for V, pi in outs]
 
-    # batched, pipelined: groups of 32 built concurrently (4 host threads, one
-    # stream each), each group solved in one launch, then freed
-    group = 32
+    # batched, pipelined: groups of 32 built (e2e_build_models; one worker: the
+    # builder already fills the GPU, and concurrent builds only add memory),
+    # each group solved in one launch, then freed
+    group, workers = 32, 1
     for V, pi in outs:
         V.fill_(float("nan"))
         pi.fill_(-7)
@@ -390,7 +391,7 @@ def run_batched(n_models: int = 256, seed: int = 2024) -> dict:
     first = None
     for g0 in range(0, n_models, group):
         tb = time.perf_counter()
-        models = api.build_models([x.prob for x in insts[g0:g0 + group]], fields[g0:g0 + group], workers=4)
+        models = api.build_models([x.prob for x in insts[g0:g0 + group]], fields[g0:g0 + group], workers=workers)
         b_build += time.perf_counter() - tb
         st1 = api.solve_batch(models, [o[0] for o in outs[g0:g0 + group]], [o[1] for o in outs[g0:g0 + group]],
                               stream=stream)
@@ -432,7 +433,7 @@ def run_batched(n_models: int = 256, seed: int = 2024) -> dict:
         "models": n_models, "states": int(sum(x.prob.ns for x in insts)), "rows": int(rows),
         "sequential_s": round(seq_s, 4), "sequential_solves_s": round(solve_s, 5),
         "batched_total_s": round(total_s, 4), "batched_build_wall_s": round(b_build, 4),
-        "batched_group": group, "build_workers": 4,
+        "batched_group": group, "build_workers": workers,
         "first_group_tune_ms": round(first["tune_ms"], 2),
         "batched_solve_s": round(batch_solve_s, 6),
         "sequential_resident_solves_s": round(seq_resident_s, 5),
@@ -555,6 +556,41 @@ def run_served(rates=(50, 200, 500, 1000, 2000), seconds_per_rate=10.0, max_requ
     }
 
 
+def run_precision() -> dict:
+    """Precision form: 300x300 grid, nt=150 (13.5 M states), 16 headings,
+    nrzns 2000, 8 modes; uint16 counts with int32 next states, FP32 values, the
+    FP64 Bellman residual of the verification sweep, and an FP64 backward solve
+    on the GPU as the check (max |V32 - V64| / max |V64|)."""
+    import torch
+
+    from e2e_gpu_dp_b200 import api
+    from e2e_gpu_dp_b200.problem import config
+    from e2e_gpu_dp_b200.workloads import device_fields
+
+    prob, spec = config("c3", seed=1234)
+    dev = device_fields(prob, spec)
+    stream = torch.cuda.current_stream()
+    V = torch.empty(prob.ns, dtype=torch.float32, device="cuda")
+    pi = torch.empty(prob.ns, dtype=torch.int32, device="cuda")
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    m = api.build_model(prob, dev, count_type="u16", stream=stream)
+    _, _, st = m.solve(method="layered", value=V, policy=pi, stream=stream)
+    torch.cuda.synchronize()
+    wall = time.perf_counter() - t0
+    _, _, chk = m.solve(method="layered", fp64_check=True, value=V, policy=pi, stream=stream)
+    inf = m.info()
+    m.free()
+    return {"workload": "300x300 grid, nt=150, 16 headings, nrzns 2000, 8 modes, uint16 counts",
+            "states": prob.ns, "rows": inf["n_rows"], "nnz": inf["nnz"],
+            "count_type": "u16" if inf["count_type"] == 0 else inf["count_type"],
+            "index_bits": inf["index_bits"], "build_kernel_ms": round(inf["build_kernel_ms"], 2),
+            "pack_ms": round(st["pack_ms"], 2), "solve_ms": round(st["seconds"] * 1e3, 3),
+            "layered_pass_ms": round(st["sweep_seconds"] * 1e3, 3), "build_solve_wall_s": round(wall, 3),
+            "fp64_residual": chk["residual"], "fp64_max_abs_err": chk["fp64_max_abs_err"],
+            "fp64_max_rel_err": chk["fp64_max_rel_err"]}
+
+
 def run_reference(args, ws, rank, local):
     if rank != 0:
         return None
@@ -650,6 +686,8 @@ def main():
     ap.add_argument("--batched-only", action="store_true", help="only the batched form (256 uneven MDPs)")
     ap.add_argument("--no-batched", action="store_true", help="skip the batched form")
     ap.add_argument("--served-only", action="store_true", help="only the served form (request server)")
+    ap.add_argument("--precision-only", action="store_true", help="only the precision form (300x300x150)")
+    ap.add_argument("--no-precision", action="store_true", help="skip the precision form")
     ap.add_argument("--no-served", action="store_true", help="skip the served form")
     args = ap.parse_args()
     if args.profile_case:
@@ -659,6 +697,9 @@ def main():
         return 0
     if args.served_only:
         print(json.dumps({"served": run_served()}), flush=True)
+        return 0
+    if args.precision_only:
+        print(json.dumps({"precision": run_precision()}), flush=True)
         return 0
     ws, rank, local = _dist()
     if args.impl == "reference":
@@ -678,6 +719,8 @@ def main():
             line["batched"] = run_batched()
         if rank == 0 and ws == 1 and not args.no_served:
             line["served"] = run_served()
+        if rank == 0 and ws == 1 and not args.no_precision:
+            line["precision"] = run_precision()
         if rank == 0:
             print(json.dumps(line), flush=True)
     finally:

@@ -89,3 +89,20 @@ def test_batch_rejects_bad_schedule(models):
     vs, ps = _outputs(models[:1])
     with pytest.raises(E2EError):
         api.solve_batch([models[0][2]], vs, ps, schedule=3 | 0x100)
+
+
+def test_concurrent_builds_equal_single_builds(models):
+    """e2e_build_models on several host threads and streams gives the same models."""
+    probs, fields = [], []
+    for name in ("t_time", "t_custom", "t_wide", "c1"):
+        p, f = problem(name)
+        probs.append(p)
+        fields.append(f)
+    built = api.build_models(probs, fields, workers=3)
+    for p, f, m in zip(probs, fields, built):
+        ref = api.build_model(p, f)
+        a, b = m.to_host(), ref.to_host()
+        for k in ("row_ptr", "col", "cnt", "R"):
+            assert np.array_equal(a[k], b[k]), (p.prob_name, k)
+        ref.free()
+        m.free()
