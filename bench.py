@@ -201,10 +201,13 @@ def run_ours(args, ws, rank, local):
     pi = torch.empty(prob.ns, dtype=torch.int32, device="cuda")
 
     def step(record=None):
+        t0 = time.perf_counter()
         m = api.build_model(prob, dev, stream=stream)
+        t1 = time.perf_counter()
         _, _, st = m.solve(method="layered", value=V, policy=pi, stream=stream)
+        t2 = time.perf_counter()
         if record is not None:
-            record.append((m.info(), st))
+            record.append((m.info(), st, (round((t1 - t0) * 1e3, 1), round((t2 - t1) * 1e3, 1))))
         m.free()
 
     for _ in range(args.warmup):
@@ -214,15 +217,19 @@ def run_ours(args, ws, rank, local):
     recs = []
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
+    marks = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps + 1)]
     with Clocks(local) as clk:
         torch.cuda.synchronize()
         e0.record(stream)
-        for _ in range(args.steps):
+        for k in range(args.steps):
             step(recs)
+            marks[k + 1].record(stream)
         e1.record(stream)
         torch.cuda.synchronize()
     _barrier(ws)
     ms = e0.elapsed_time(e1) / args.steps
+    step_ms = [round(e0.elapsed_time(marks[1]), 2)] + [round(marks[k].elapsed_time(marks[k + 1]), 2)
+                                                        for k in range(1, args.steps)]
     ms = _max_over_ranks(ms, ws)
     clocks = clk.summary()
 
@@ -273,6 +280,29 @@ def run_ours(args, ws, rank, local):
     vi_gbs = jst["stream_bytes_per_sweep"] * jst["iterations"] / jst["seconds"] / 1e9
     vi_csr_gbs = jst["bytes_per_sweep"] * jst["iterations"] / jst["seconds"] / 1e9
 
+    # policy rollout evaluation of the solved c2 policy from the reference
+    # script's start cell (int(0.5 g), int(0.95 g)), every realisation, against
+    # the Python restatement of the reference's trajectory loop on a sample
+    start = (int(0.5 * prob.gsize), int(0.95 * prob.gsize))
+    m = api.build_model(prob, dev, stream=stream)
+    m.solve(method="layered", value=V, policy=pi, stream=stream)
+    m.free()
+    ro = api.rollout(prob, dev, pi, start, stream=stream)
+    ro2 = api.rollout(prob, dev, pi, start, stream=stream)
+    rollout = {"start": list(start), "realisations": prob.nrzns, "success_rate": ro2["stats"]["success_rate"],
+               "mean_time": ro2["stats"]["mean_time"], "kernel_s": round(ro2["stats"]["seconds"], 6)}
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        from oracle import rollout as RO
+        pih = pi.cpu().numpy().astype(np.int64)
+        n_cpu = 100
+        tc = time.perf_counter()
+        o = RO.rollout(prob, fields, pih, start, n_rzns=n_cpu, dot="numpy")
+        cpu_s = (time.perf_counter() - tc) / n_cpu * prob.nrzns
+        same = float(np.mean(o["success"] == ro2["success"][:n_cpu]))
+        rollout.update({"cpu_reference_loop_s_extrapolated": round(cpu_s, 3), "cpu_sample": n_cpu,
+                        "outcome_agreement_on_sample": same,
+                        "speedup_vs_cpu": round(cpu_s / max(ro2["stats"]["seconds"], 1e-9), 1)})
+
     cb = 2 if info["count_type"] == 0 else 4
     k1_bytes = algorithmic_build_bytes(prob, info["nnz"], cb)
     k1_gbs = k1_bytes / (k1_ms * 1e-3) / 1e9
@@ -309,6 +339,7 @@ def run_ours(args, ws, rank, local):
         "e2e": {"value": round(e2e_ms / 1e3 / ws, 6), "unit": "s", "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": d2h},
         "gpu_launches": launches,
+        "step_ms": step_ms, "step_host_ms": [r[2] for r in recs],
         "phases_ms": {"build_kernel": round(k1_ms, 3), "assemble": round(asm_ms, 3),
                       "pack": round(pack_ms, 3), "solve": round(solve_ms, 3),
                       "layered_pass": round(pass_ms, 3)},
@@ -326,6 +357,7 @@ def run_ours(args, ws, rank, local):
                "layered_seconds": round(lst["seconds"], 6),
                "layered_pass_seconds": round(lst["sweep_seconds"], 6),
                "fp64_max_rel_err": lst["fp64_max_rel_err"]},
+        "rollout": rollout,
         "clocks": clocks,
     }
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
@@ -644,6 +676,7 @@ def run_reference(args, ws, rank, local):
                                    "of build_model + int32 convert + spvi_2"},
         "e2e": {"value": round(value, 4), "unit": "s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
+        "rollout": rollout,
         "clocks": clocks,
     }
 

@@ -104,6 +104,17 @@ class ServerStats(C.Structure):
                 ("solve_ms", C.c_double)]
 
 
+class RolloutOpts(C.Structure):
+    _fields_ = [("i_start", C.c_int32), ("j_start", C.c_int32), ("n_rzns", C.c_int32), ("reserved", C.c_int32)]
+
+
+class RolloutStats(C.Structure):
+    _fields_ = [("n", C.c_int32), ("successes", C.c_int32), ("failures", C.c_int32), ("undecided", C.c_int32),
+                ("invalid", C.c_int32), ("reserved", C.c_int32), ("success_rate", C.c_double),
+                ("mean_time", C.c_double), ("mean_energy_cons", C.c_double), ("mean_energy_col", C.c_double),
+                ("mean_net_energy", C.c_double), ("seconds", C.c_double)]
+
+
 # every exported symbol of include/e2e_dp.h with its signature
 SIGNATURES = {
     "e2e_abi_version": (C.c_int, []),
@@ -130,6 +141,9 @@ SIGNATURES = {
                                        C.POINTER(BatchStats), C.c_void_p]),
     "e2e_build_models": (C.c_int, [C.POINTER(Problem), C.POINTER(Fields), C.c_int32, C.c_int,
                                    C.POINTER(BuildOpts), C.c_int32, C.POINTER(C.c_void_p)]),
+    "e2e_rollout": (C.c_int, [C.POINTER(Problem), C.POINTER(Fields), C.c_int, C.c_void_p, C.c_int,
+                              C.POINTER(RolloutOpts), C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                              C.POINTER(RolloutStats), C.c_void_p]),
     "e2e_server_create": (C.c_int, [C.POINTER(ServerOpts), C.POINTER(C.c_void_p)]),
     "e2e_server_add_field": (C.c_int, [C.c_void_p, C.POINTER(Problem), C.POINTER(Fields), C.c_int,
                                        C.POINTER(C.c_int32)]),

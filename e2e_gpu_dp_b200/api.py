@@ -270,3 +270,32 @@ class Server:
             self.close()
         except Exception:
             pass
+
+
+def rollout(prob: Problem, fields: Dict, policy, start, n_rzns: int = 0, stream=None) -> Dict:
+    """Follow ``policy`` (ns int32, numpy or CUDA tensor) from ``start`` (i, j)
+    for each realisation (e2e_rollout).  Returns per-realisation arrays and
+    the summary of the reference's get_metrics."""
+    where, f, keep = _fields_ptrs(fields)
+    n = n_rzns if n_rzns > 0 else prob.nrzns
+    if _is_device(policy):
+        pw, pptr = _lib.E2E_DEVICE, policy.data_ptr()
+    else:
+        pol = np.ascontiguousarray(policy, dtype=np.int32)
+        keep.append(pol)
+        pw, pptr = _lib.E2E_HOST, pol.ctypes.data
+    succ = np.empty(n, np.int8)
+    tt = np.empty(n, np.int32)
+    en = np.empty((n, 3), np.float32)
+    fin = np.empty((n, 3), np.int32)
+    o = _lib.RolloutOpts(int(start[0]), int(start[1]), n, 0)
+    st = _lib.RolloutStats()
+    cp = c_problem(prob)
+    check(lib().e2e_rollout(C.byref(cp), C.byref(f), where, pptr, pw, C.byref(o), succ.ctypes.data,
+                            tt.ctypes.data, en.ctypes.data, fin.ctypes.data, C.byref(st), _stream_ptr(stream)))
+    del keep
+    out = {"success": succ, "travel_time": tt, "energy_cons": en[:, 0].astype(np.float64),
+           "energy_col": en[:, 1].astype(np.float64), "net_energy": en[:, 2].astype(np.float64),
+           "final_tij": fin}
+    out["stats"] = {k: getattr(st, k) for k, _ in _lib.RolloutStats._fields_}
+    return out

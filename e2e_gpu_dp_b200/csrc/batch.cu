@@ -6,7 +6,8 @@
 //
 // The device job table has a fixed capacity, so the graph's nodes never
 // change: a copy of the pinned host table into the device table, a reset of
-// the grid-barrier words, and the kernel.  A new batch rewrites the pinned
+// the error word and of the per-(job, layer) completion counters, and the
+// kernel.  A new batch rewrites the pinned
 // host table and replays the graph.  The schedule (warps per chunk, kernel
 // variant and L2 prefetch) is picked per batch shape by timing the
 // candidates on the first batch of that shape.
@@ -48,18 +49,21 @@ class BatchSolver {
   int device = -1;
   void* d_table = nullptr;
   unsigned char* h_table = nullptr;
-  unsigned int* d_sync = nullptr;
+  unsigned int* d_sync = nullptr;  // [1]: error bits of the bounded waits
+  int* d_done = nullptr;           // [kJobCap][kLayerCap] chunks finished per (job, layer)
   cudaStream_t priv = nullptr;
   cudaEvent_t ev_in = nullptr, ev_out = nullptr, t0 = nullptr, t1 = nullptr;
   std::map<std::tuple<int, int, int, int, int>, cudaGraphExec_t> graphs;  // mode, cnt, G, tune, grid
   std::map<std::tuple<int, int, int, int>, Choice> tuned;                // mode, cnt, log2 jobs, log2 items
   size_t table_bytes = vi_batch_table_bytes(kJobCap, kLayerCap);
+  size_t done_bytes = sizeof(int) * (size_t)kJobCap * kLayerCap;
 
   e2e_status init(int dev) {
     if (device == dev) return E2E_OK;
     if (device >= 0) return fail(E2E_ERR_UNSUPPORTED, "batch solver bound to another device");
     CK(dalloc(&d_table, table_bytes, nullptr));
     CK(dalloc((void**)&d_sync, sizeof(unsigned int) * 2, nullptr));
+    CK(dalloc((void**)&d_done, done_bytes, nullptr));
     CK(cudaHostAlloc((void**)&h_table, table_bytes, cudaHostAllocDefault));
     std::memset(h_table, 0, table_bytes);
     CK(cudaStreamCreateWithFlags(&priv, cudaStreamNonBlocking));
@@ -85,7 +89,10 @@ class BatchSolver {
         CK(cudaStreamBeginCapture(priv, cudaStreamCaptureModeThreadLocal));
         cudaError_t e = cudaMemcpyAsync(d_table, h_table, table_bytes, cudaMemcpyHostToDevice, priv);
         if (e == cudaSuccess) e = cudaMemsetAsync(d_sync, 0, sizeof(unsigned int) * 2, priv);
-        if (e == cudaSuccess) e = launch_vi_batch(d_table, kJobCap, mode, cnt, ch.groups, grid, ch.tune, d_sync, priv);
+        if (e == cudaSuccess) e = cudaMemsetAsync(d_done, 0, done_bytes, priv);
+        if (e == cudaSuccess)
+          e = launch_vi_batch(d_table, kJobCap, kLayerCap, mode, cnt, ch.groups, grid, ch.tune, d_done, d_sync + 1,
+                              priv);
         cudaError_t e2 = cudaStreamEndCapture(priv, &g);
         if (e == cudaSuccess && e2 == cudaSuccess) e = cudaGraphInstantiate(&ge, g, 0);
         if (g) cudaGraphDestroy(g);
@@ -108,7 +115,8 @@ class BatchSolver {
     }
     CK(cudaMemcpyAsync(d_table, h_table, table_bytes, cudaMemcpyHostToDevice, st));
     CK(cudaMemsetAsync(d_sync, 0, sizeof(unsigned int) * 2, st));
-    CK(launch_vi_batch(d_table, kJobCap, mode, cnt, ch.groups, grid, ch.tune, d_sync, st));
+    CK(cudaMemsetAsync(d_done, 0, done_bytes, st));
+    CK(launch_vi_batch(d_table, kJobCap, kLayerCap, mode, cnt, ch.groups, grid, ch.tune, d_done, d_sync + 1, st));
     return E2E_OK;
   }
 
@@ -116,7 +124,7 @@ class BatchSolver {
     unsigned int h[2] = {0, 0};
     CK(cudaMemcpyAsync(h, d_sync, sizeof(h), cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
-    if (h[1]) return fail(E2E_ERR_DEVICE, "a bounded grid barrier of the batched sweep gave up");
+    if (h[1]) return fail(E2E_ERR_DEVICE, "a bounded wait of the batched sweep gave up");
     return E2E_OK;
   }
 };

@@ -157,13 +157,15 @@ struct ViBatchHeader {
 // Device table: header | jobs[job_cap] | cum[job_cap + 1] | nact[layer_cap].
 // Jobs sorted by nlayers, descending; cum = prefix sums of their chunks per
 // layer; nact[k] = jobs with more than k layers.  Step k of the launch works
-// on layer nlayers-1-k of jobs [0, nact[k]): chunk items [0, cum[nact[k]]).
+// on layer nlayers-1-k of jobs [0, nact[k]): chunk items [0, cum[nact[k]]),
+// each waiting only for its own job's next layer.
 size_t vi_batch_table_bytes(int job_cap, int layer_cap);
 constexpr size_t kViBatchJobsOffset = 64;  // header padded to 64 bytes
 // CTAs of the batch kernel that fit on the device at once
 int vi_batch_capacity(int ent_mode, int count_type, int tune);
-// sync: two zeroed words; grid <= vi_batch_capacity (co-resident CTAs)
-cudaError_t launch_vi_batch(const void* table, int job_cap, int ent_mode, int count_type, int groups,
-                            int grid, int tune, unsigned int* sync, cudaStream_t st);
+// done: zeroed [job_cap][layer_cap] completion counters; err: zeroed error word;
+// grid <= vi_batch_capacity (co-resident CTAs)
+cudaError_t launch_vi_batch(const void* table, int job_cap, int layer_cap, int ent_mode, int count_type,
+                            int groups, int grid, int tune, int* done, unsigned int* err, cudaStream_t st);
 
 }  // namespace e2e

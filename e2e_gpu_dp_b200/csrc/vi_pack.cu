@@ -65,6 +65,12 @@ __device__ __forceinline__ unsigned int ld_acquire(const unsigned int* p) {
   return v;
 }
 
+__device__ __forceinline__ int ld_acquire_s32(const int* p) {
+  int v;
+  asm volatile("ld.acquire.gpu.global.s32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+
 template <typename T>
 __device__ __forceinline__ T ld_stream(const T* p) {
   return __ldcs(p);
@@ -395,10 +401,16 @@ __global__ void __launch_bounds__(kThreads, MinBlocks<MODE, VAR>::value)
   }
 }
 
-// Many layered solves in one persistent launch.  Step k works on layer
+// Many layered solves in one persistent launch.  Step k covers layer
 // nlayers-1-k of every job that has more than k layers (jobs sorted by layer
-// count, so those are a prefix and their chunks a contiguous item range);
-// a grid barrier separates the steps.  Jobs with a target take R of the
+// count, so those are a prefix and their chunks a contiguous item range).
+// There is no grid-wide barrier: a chunk of layer t waits only until its own
+// job's layer t+1 is complete (done[job][t+1] == chunks per layer), and each
+// finished chunk adds one to done[job][t].  Every CTA takes its items in step
+// order and all CTAs are resident (cooperative launch), so each wait is for
+// items of an earlier step that are finished or running; the waits are
+// bounded and a timeout sets bit 2 of err and lets the rest drain quickly.
+// Jobs with a target take R of the
 // cells around it from their Rwin table, and the target's own cells are
 // terminal: the reference leaves such a sample in place with reward 0
 // (src/build_model.cu:523-545), i.e. one entry (the cell at t+1, count
@@ -410,7 +422,8 @@ struct BatchMinBlocks {  // the job lookup needs a few more registers than k_vi_
 
 template <int MODE, typename CntT, int VAR>
 __global__ void __launch_bounds__(kThreads, BatchMinBlocks<MODE, VAR>::value)
-    k_vi_batch(const unsigned char* table, int job_cap, int groups, unsigned int* sync, int prefetch) {
+    k_vi_batch(const unsigned char* table, int job_cap, int groups, int* done, int layer_cap,
+               unsigned int* err, int prefetch) {
   __shared__ float sq[kWarps][32];
   __shared__ int sa[kWarps][32];
   const ViBatchHeader* H = reinterpret_cast<const ViBatchHeader*>(table);
@@ -421,7 +434,6 @@ __global__ void __launch_bounds__(kThreads, BatchMinBlocks<MODE, VAR>::value)
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   const int cpc = kWarps / groups;
   const int grp = wid % groups, slot_in_cta = wid / groups;
-  unsigned int gen = 0;
   for (int k = 0; k < L; ++k) {
     const int nj = nact[k];
     const int n_items = cum[nj];
@@ -434,6 +446,8 @@ __global__ void __launch_bounds__(kThreads, BatchMinBlocks<MODE, VAR>::value)
       float* Vout = nullptr;
       int32_t* pout = nullptr;
       int64_t s_out = 0;
+      int* done_slot = nullptr;
+      bool skip = false;
       if (active) {
         int lo = 0, hi = nj - 1;  // last job with cum[job] <= item
         while (lo < hi) {
@@ -445,12 +459,36 @@ __global__ void __launch_bounds__(kThreads, BatchMinBlocks<MODE, VAR>::value)
         const ViPack& P = J.P;
         const int na = P.na;
         const int apg = (na + groups - 1) / groups;
-        const int a0 = min(na, grp * apg), a1 = min(na, a0 + apg);
+        int a0 = min(na, grp * apg);
+        const int a1 = min(na, a0 + apg);
         const int cpl = (int)P.cpl, nc = (int)P.nc;
         const int t = P.nlayers - 1 - k;
         const int c = t * cpl + (item - __ldg(cum + lo));
+        done_slot = done + (int64_t)lo * layer_cap + t;
         if ((prefetch & PF_NEXT) && lane == 0 && grp == 0 && t > 0)
           prefetch_chunk(P, c - cpl, Widths<MODE, CntT>::col, Widths<MODE, CntT>::cnt);
+        if (t + 1 < P.nlayers) {  // layer t+1 of this job complete
+          const int* dep = done_slot + 1;
+          int ok = 1;
+          if (lane == 0) {
+            const unsigned long long t0 = global_ns();
+            long long it = 0;
+            while (ld_acquire_s32(dep) < cpl) {
+              if (ld_acquire(err) != 0u || ++it > kBarrierSpinLimit || global_ns() - t0 > kBarrierTimeoutNs) {
+                atomicOr(err, 4u);
+                ok = 0;
+                break;
+              }
+              __nanosleep(64);
+            }
+          }
+          ok = __shfl_sync(0xffffffffu, ok, 0);
+          (void)ld_acquire_s32(dep);  // every lane orders its reads after the producers' writes
+          if (!ok) {
+            skip = true;  // give up this chunk: nothing computed, nothing written
+            a0 = a1;
+          }
+        }
         const ChunkPos cp = chunk_pos(P, c, lane, MODE != ENT_I32);
         const float* Rp = pack_r(P, c, a0, lane);
         int rstride = 32;
@@ -477,7 +515,7 @@ __global__ void __launch_bounds__(kThreads, BatchMinBlocks<MODE, VAR>::value)
             ba = a0;
           }
         }
-        valid = cp.valid;
+        valid = cp.valid && !skip;
         Vout = J.V;
         pout = J.pi;
         s_out = cp.s;
@@ -497,17 +535,20 @@ __global__ void __launch_bounds__(kThreads, BatchMinBlocks<MODE, VAR>::value)
         }
         __syncthreads();
       }
-      if (active && grp == 0 && valid) {
-        float vout;
-        int32_t po;
-        finish_state(bq, ba, vout, po);
-        Vout[s_out] = vout;
-        pout[s_out] = po;
+      if (active && grp == 0) {
+        if (valid) {
+          float vout;
+          int32_t po;
+          finish_state(bq, ba, vout, po);
+          Vout[s_out] = vout;
+          pout[s_out] = po;
+        }
+        __syncwarp();
+        if (lane == 0) {
+          __threadfence();  // this chunk's values before its completion count
+          atomicAdd(done_slot, 1);
+        }
       }
-    }
-    if (k + 1 < L) {
-      ++gen;
-      if (!grid_barrier(sync, gen * gridDim.x)) return;
     }
   }
 }
@@ -830,8 +871,8 @@ int vi_batch_capacity(int ent_mode, int count_type, int tune) {
   return cap;
 }
 
-cudaError_t launch_vi_batch(const void* table, int job_cap, int ent_mode, int count_type, int groups,
-                            int grid, int tune, unsigned int* sync, cudaStream_t st) {
+cudaError_t launch_vi_batch(const void* table, int job_cap, int layer_cap, int ent_mode, int count_type,
+                            int groups, int grid, int tune, int* done, unsigned int* err, cudaStream_t st) {
   if (groups != 1 && groups != 2 && groups != 4 && groups != 8) return cudaErrorInvalidValue;
   const int prefetch = tune & (PF_NEXT | PF_CURRENT);
   return dispatch_key(PackKey{ent_mode, count_type}, [&](auto mode, auto* cntt) -> cudaError_t {
@@ -853,7 +894,7 @@ cudaError_t launch_vi_batch(const void* table, int job_cap, int ent_mode, int co
     cfg.numAttrs = 1;
     const unsigned char* tb = reinterpret_cast<const unsigned char*>(table);
     int pf = prefetch;
-    return cudaLaunchKernelEx(&cfg, kern, tb, job_cap, groups, sync, pf);
+    return cudaLaunchKernelEx(&cfg, kern, tb, job_cap, groups, done, layer_cap, err, pf);
   });
 }
 

@@ -309,6 +309,37 @@ e2e_status e2e_server_fetch(e2e_server* s, int64_t request_id, float* value_out,
 e2e_status e2e_server_get_stats(e2e_server* s, e2e_server_stats* out);
 e2e_status e2e_server_destroy(e2e_server* s);
 
+/* ---- policy rollout evaluation ------------------------------------------------
+ * Replaces the reference's Python trajectory loop (Post_processing/
+ * plot_e2eGPU_policy.py:433-474, plot_exact_trajectory_set_DP without policy
+ * interpolation, moving with Grid.move_exact, grid_world.py:160-271) and
+ * get_metrics (:776-797): one GPU thread follows the policy from the start cell
+ * for each realisation of the velocity field, on continuous positions, until
+ * the target (terminal subgrid of p), an edge or obstacle cell, or the last
+ * step.  Float32 arithmetic as the reference under NumPy's scalar rules; the
+ * mode sum of the velocity is a sequential fma chain. */
+typedef struct {
+  int32_t i_start, j_start; /* start cell at t = 0 */
+  int32_t n_rzns;           /* realisations to follow (0 = all of the field's) */
+  int32_t reserved;
+} e2e_rollout_opts;
+
+typedef struct {
+  int32_t n, successes, failures, undecided, invalid; /* invalid: the policy had no action there */
+  int32_t reserved;
+  double success_rate;
+  double mean_time, mean_energy_cons, mean_energy_col, mean_net_energy; /* over successes */
+  double seconds;           /* device time of the rollout kernel */
+} e2e_rollout_stats;
+
+/* policy: ns int32 (host or device); outputs (host, each may be NULL): success
+ * int8 per realisation (1 target, 0 failed, -1 undecided, -2 invalid policy),
+ * travel time int32, energies float32 x3 (sum F^2, sum mean scalar field, their
+ * difference), final (t, i, j) int32 x3. */
+e2e_status e2e_rollout(const e2e_problem* p, const e2e_fields* f, int fields_where, const int32_t* policy,
+                       int policy_where, const e2e_rollout_opts* opts, int8_t* success_out, int32_t* time_out,
+                       float* energy_out, int32_t* final_out, e2e_rollout_stats* stats, void* stream);
+
 /* ---- solve without device allocation ----------------------------------------
  * No counterpart in the reference.  For callers that cannot allocate device
  * memory (a serving loop whose memory is fully reserved by its own pool, or code
