@@ -46,23 +46,63 @@ def _peaks():
 
 
 class Clocks:
-    """nvidia-smi sampler over the timed region (200 ms period)."""
+    """SM clock and clock-event-reason samples over the timed region.
 
+    NVML in this process, initialised before the region starts.  Samples are
+    taken at step boundaries (``tick``, right after each step's last
+    synchronisation, clocks still at their load level) and never while a
+    kernel runs: NVML queries issued during the builder's long launches (a
+    sampler thread, or nvidia-smi started inside the region) blocked the
+    host's CUDA calls and added 0.2-0.7 s to some steps.  nvidia-smi at a
+    200 ms period when NVML is absent."""
+
+    # clock event reason bits of NVML (nvmlClocksEventReason*)
+    REASONS = {"sw_power_cap": 0x4, "hw_slowdown": 0x8, "sw_thermal_slowdown": 0x20,
+               "hw_thermal_slowdown": 0x40}
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
          "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
          "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
     def __init__(self, device_index: int):
         self.dev = device_index
+        self.samples = []
         self.proc = None
         self.path = None
+        self.thread = None
+
+    def _uuid(self):
+        import torch
+
+        uuid = str(torch.cuda.get_device_properties(self.dev).uuid)
+        return uuid if uuid.startswith("GPU-") else "GPU-" + uuid
+
+    def _sample(self, nv, h):
+        sm = nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)
+        smax = nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM)
+        try:
+            reasons = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
+        except AttributeError:
+            reasons = nv.nvmlDeviceGetCurrentClocksThrottleReasons(h)
+        self.samples.append((float(sm), float(smax), int(reasons)))
 
     def __enter__(self):
         try:
-            import torch
+            import pynvml as nv
 
-            uuid = str(torch.cuda.get_device_properties(self.dev).uuid)
-            sel = ["-i", "GPU-" + uuid if not uuid.startswith("GPU-") else uuid]
+            nv.nvmlInit()
+            try:
+                h = nv.nvmlDeviceGetHandleByUUID(self._uuid())
+            except Exception:
+                h = nv.nvmlDeviceGetHandleByIndex(self.dev)
+            self._sample(nv, h)      # first query outside the timed region
+            self.samples.clear()
+            self._nv, self._h = nv, h
+            self.thread = True       # NVML mode
+            return self
+        except Exception:
+            self.thread = None
+        try:
+            sel = ["-i", self._uuid()]
         except Exception:
             sel = ["-i", str(self.dev)]
         fd, self.path = tempfile.mkstemp(suffix=".csv")
@@ -71,10 +111,20 @@ class Clocks:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", *sel, f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
                  "-lms", "200"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
-            time.sleep(0.3)
+            t0 = time.time()
+            while time.time() - t0 < 10 and os.path.getsize(self.path) == 0:
+                time.sleep(0.05)   # its first sample is taken before timing starts
         except Exception:
             self.proc = None
         return self
+
+    def tick(self):
+        """One sample (NVML mode), called between steps."""
+        if self.thread is not None:
+            try:
+                self._sample(self._nv, self._h)
+            except Exception:
+                pass
 
     def __exit__(self, *a):
         if self.proc is not None:
@@ -86,28 +136,35 @@ class Clocks:
                 self.proc.kill()
 
     def summary(self):
-        if not self.path or not os.path.exists(self.path):
-            return None
         sm, smax, reasons = [], [], set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        with open(self.path) as fh:
-            for line in fh:
-                parts = [p.strip() for p in line.split(",")]
-                if len(parts) < 9:
-                    continue
-                try:
-                    sm.append(float(parts[1]))
-                    smax.append(float(parts[2]))
-                except ValueError:
-                    continue
-                for n, v in zip(names, parts[5:9]):
-                    if v.lower().startswith("active"):
+        if self.thread is not None:
+            for a, b, r in self.samples:
+                sm.append(a)
+                smax.append(b)
+                for n, bit in self.REASONS.items():
+                    if r & bit:
                         reasons.add(n)
-        os.unlink(self.path)
+        elif self.path and os.path.exists(self.path):
+            names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+            with open(self.path) as fh:
+                for line in fh:
+                    parts = [p.strip() for p in line.split(",")]
+                    if len(parts) < 9:
+                        continue
+                    try:
+                        sm.append(float(parts[1]))
+                        smax.append(float(parts[2]))
+                    except ValueError:
+                        continue
+                    for n, v in zip(names, parts[5:9]):
+                        if v.lower().startswith("active"):
+                            reasons.add(n)
+            os.unlink(self.path)
         if not sm:
             return None
         return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(smax),
-                "reasons": sorted(reasons), "samples": len(sm)}
+                "reasons": sorted(reasons), "samples": len(sm),
+                "source": "nvml" if self.thread is not None else "nvidia-smi"}
 
 
 def _dist():
@@ -224,6 +281,8 @@ def run_ours(args, ws, rank, local):
         for k in range(args.steps):
             step(recs)
             marks[k + 1].record(stream)
+            torch.cuda.synchronize()
+            clk.tick()
         e1.record(stream)
         torch.cuda.synchronize()
     _barrier(ws)
@@ -264,8 +323,11 @@ def run_ours(args, ws, rank, local):
     f0 = torch.cuda.Event(enable_timing=True)
     f1 = torch.cuda.Event(enable_timing=True)
     f0.record(stream)
+    e2e_steps = []
     for _ in range(args.steps):
+        te = time.perf_counter()
         e2e_step()
+        e2e_steps.append(round((time.perf_counter() - te) * 1e3, 1))
     f1.record(stream)
     torch.cuda.synchronize()
     e2e_ms = max(f0.elapsed_time(f1), (time.perf_counter() - t0) * 1e3) / args.steps
@@ -337,7 +399,7 @@ def run_ours(args, ws, rank, local):
             "parallelism": f"replicas x{ws}", "l2": "inputs (fields 0.45 GB, model 2.2 GB) exceed L2",
         },
         "e2e": {"value": round(e2e_ms / 1e3 / ws, 6), "unit": "s", "h2d_bytes_per_step": h2d,
-                "d2h_bytes_per_step": d2h},
+                "d2h_bytes_per_step": d2h, "step_wall_ms": e2e_steps},
         "gpu_launches": launches,
         "step_ms": step_ms, "step_host_ms": [r[2] for r in recs],
         "phases_ms": {"build_kernel": round(k1_ms, 3), "assemble": round(asm_ms, 3),
@@ -708,6 +770,32 @@ def profile_case():
     return 0
 
 
+def profile_batch():
+    """Small case of the batched sweep for ncu: 32 of the batched form's
+    problems with grid <= 96 (a few GB on the device), built, then solved in
+    one direct launch with a fixed schedule (one warp per chunk, lean kernel,
+    no prefetch)."""
+    import torch
+
+    from e2e_gpu_dp_b200 import api
+    from e2e_gpu_dp_b200.workloads import batch_instances, device_fields
+
+    insts = [x for x in batch_instances(256) if x.prob.gsize <= 96][:32]
+    fields = [device_fields(x.prob, x.spec) for x in insts]
+    models = api.build_models([x.prob for x in insts], fields)
+    outs = [(torch.empty(x.prob.ns, dtype=torch.float32, device="cuda"),
+             torch.empty(x.prob.ns, dtype=torch.int32, device="cuda")) for x in insts]
+    sch = 1 | (4 << 4) | 0x100 | 0x200
+    st = api.solve_batch(models, [o[0] for o in outs], [o[1] for o in outs], schedule=sch)
+    st = api.solve_batch(models, [o[0] for o in outs], [o[1] for o in outs], schedule=sch)
+    print(json.dumps({"profile_batch": len(insts), "rows": int(sum((x.prob.nt - 1) * x.prob.ncells *
+                                                                    x.prob.num_actions for x in insts)),
+                      "stream_bytes": st["stream_bytes"], "seconds": st["seconds"]}))
+    for m in models:
+        m.free()
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -716,6 +804,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--profile-case", action="store_true", help="small case for ncu captures")
+    ap.add_argument("--profile-batch", action="store_true", help="small batched case for ncu captures")
     ap.add_argument("--batched-only", action="store_true", help="only the batched form (256 uneven MDPs)")
     ap.add_argument("--no-batched", action="store_true", help="skip the batched form")
     ap.add_argument("--served-only", action="store_true", help="only the served form (request server)")
@@ -725,6 +814,8 @@ def main():
     args = ap.parse_args()
     if args.profile_case:
         return profile_case()
+    if args.profile_batch:
+        return profile_batch()
     if args.batched_only:
         print(json.dumps({"batched": run_batched()}), flush=True)
         return 0

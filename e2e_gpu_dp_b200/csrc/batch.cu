@@ -9,7 +9,7 @@
 // the error word and of the per-(job, layer) completion counters, and the
 // kernel.  A new batch rewrites the pinned
 // host table and replays the graph.  The schedule (warps per chunk, kernel
-// variant and L2 prefetch) is picked per batch shape by timing the
+// variant and L2 prefetch) is picked per batch shape by timing the 16
 // candidates on the first batch of that shape.
 #include <cuda_runtime.h>
 
@@ -150,10 +150,11 @@ e2e_status solve_batch(const std::vector<BatchJobSpec>& jobs, int schedule, cuda
   *res = BatchResult{};
   if (jobs.empty()) return E2E_OK;
   const int gsel = schedule & 15;
-  if ((schedule & ~0x37f) || (gsel != 0 && gsel != 1 && gsel != 2 && gsel != 4 && gsel != 8))
+  if ((schedule & ~0x77f) || (gsel != 0 && gsel != 1 && gsel != 2 && gsel != 4 && gsel != 8))
     return fail(E2E_ERR_INVALID, "schedule: bits 0-3 warps per chunk (0, 1, 2, 4, 8), bits 4-6 tuning, "
-                                 "bit 8 tuning given, bit 9 no CUDA graph");
+                                 "bit 8 tuning given, bit 9 no CUDA graph, bit 10 heuristic schedule");
   const bool tune_given = (schedule & 0x100) != 0;
+  const bool heuristic = (schedule & 0x400) != 0;
   const bool use_graph = (schedule & 0x200) == 0;
   for (const auto& j : jobs) {
     if (!j.m || !j.V || !j.pi) return fail(E2E_ERR_INVALID, "batch job without model or outputs");
@@ -194,6 +195,7 @@ e2e_status solve_batch(const std::vector<BatchJobSpec>& jobs, int schedule, cuda
       int* nact = cum + kJobCap + 1;
       int maxL = 0, min_na = 1 << 30;
       int64_t total = 0;
+      double step_bytes = 0;  // one layer of every job
       cum[0] = 0;
       for (int q = 0; q < n; ++q) {
         const BatchJobSpec& js = jobs[idx[off + q]];
@@ -216,6 +218,7 @@ e2e_status solve_batch(const std::vector<BatchJobSpec>& jobs, int schedule, cuda
         maxL = std::max(maxL, P.nlayers);
         min_na = std::min(min_na, P.na);
         res->stream_bytes += pack_sweep_bytes(P);
+        step_bytes += (double)pack_sweep_bytes(P) / P.nlayers;
       }
       for (int k = 0; k < maxL; ++k) {
         int a = 0;
@@ -234,6 +237,12 @@ e2e_status solve_batch(const std::vector<BatchJobSpec>& jobs, int schedule, cuda
       if (tune_given) {
         ch.tune = (schedule >> 4) & 7;
         ch.groups = gsel;
+      } else if (heuristic) {
+        // no timing runs (request paths): prefetch the next layer while a step's
+        // data fits well inside L2; the lean kernel once a step fills the GPU
+        const int cap = vi_batch_capacity(mode, cnt, VI_TUNE_LEAN);
+        ch.tune = (step_bytes < 48e6 ? VI_TUNE_PF_NEXT : 0) | (total >= (int64_t)cap * 8 * 2 ? VI_TUNE_LEAN : 0);
+        ch.groups = gsel;
       } else {
         const auto key = std::make_tuple(mode, cnt, ilog2(n), ilog2(total / std::max(1, n) + 1));
         auto it = S.tuned.find(key);
@@ -245,7 +254,10 @@ e2e_status solve_batch(const std::vector<BatchJobSpec>& jobs, int schedule, cuda
           float best = 1e30f;
           for (int G : {1, 2, 4, 8}) {
             if (G > min_na) continue;
-            for (int tn : {(int)VI_TUNE_PF_NEXT, (int)(VI_TUNE_PF_NEXT | VI_TUNE_LEAN)}) {
+            // with and without the L2 prefetch of the next layer: it pays while
+            // a step's data fits L2 and costs bandwidth (evicted, read twice)
+            // when it does not
+            for (int tn : {(int)VI_TUNE_PF_NEXT, (int)(VI_TUNE_PF_NEXT | VI_TUNE_LEAN), 0, (int)VI_TUNE_LEAN}) {
               Choice c{G, tn};
               bool gr = false;
               cudaEvent_t a, b;

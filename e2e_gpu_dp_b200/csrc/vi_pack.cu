@@ -78,9 +78,12 @@ __device__ __forceinline__ T ld_stream(const T* p) {
 
 template <bool COHERENT>
 __device__ __forceinline__ float ld_value(const float* p) {
-  // V written by other CTAs of the same persistent launch must not come from
-  // a stale L1 line: read it at L2.
-  if (COHERENT) return __ldcg(p);
+  // V written by other CTAs of the same persistent launch: an ordinary
+  // (weak, L1-cached) load, never the read-only path.  Every reader is
+  // ordered after an acquire of the completion that released those writes
+  // (grid barrier, or its own acquire of the layer counter), so the memory
+  // model makes it observe them.
+  if (COHERENT) return *p;  // not const __restrict__: the compiler keeps the coherent path
   return __ldg(p);
 }
 
@@ -505,7 +508,7 @@ __global__ void __launch_bounds__(kThreads, BatchMinBlocks<MODE, VAR>::value)
         }
         chunk_best<MODE, CntT, true, VAR>(P, c, cp, lane, a0, a1, J.V, bq, ba, Rp, rstride);
         if (terminal) {
-          const float v = __ldcg(J.V + cp.s + nc);  // the same cell, layer t+1
+          const float v = ld_value<true>(J.V + cp.s + nc);  // the same cell, layer t+1
           const float acc = fmaf((float)P.nrzns, v, 0.f);
           const float q = finish_row(0.f, acc, 0.f, P.nrzns, true);
           bq = -INFINITY;

@@ -222,8 +222,10 @@ e2e_status e2e_spvi_solve(const e2e_model* m, const e2e_vi_opts* opts /* may be 
  * last layer), captured in a CUDA graph that later batches of the same launch
  * shape replay.  Results are bit-identical to e2e_spvi_solve(method = 1) on each
  * model.  value_dev[i] / policy_dev[i]: device buffers of model i's ns states.
- * opts->schedule as for e2e_spvi_solve, plus bit 9: launch directly, no graph;
- * without bit 8 the schedule is autotuned on the first batch of each shape.
+ * opts->schedule as for e2e_spvi_solve, plus bit 9: launch directly, no graph,
+ * and bit 10: pick the schedule by a rule (no timing runs); without bits 8 and
+ * 10 the schedule (warps per chunk, kernel variant, L2 prefetch) is autotuned
+ * on the first batch of each shape.
  * Calls are serialised inside the library. */
 /* Builds n problems (problems[i] with fields[i], all in fields_where memory)
  * with e2e_build_model on `workers` host threads, each with its own stream
@@ -264,7 +266,7 @@ typedef struct e2e_server e2e_server;
 typedef struct {
   int64_t hbm_budget;  /* bytes for models and requests; 0 = 80% of the free memory at creation */
   int32_t max_batch;   /* requests per launch; 0 = 256 (at most 1024) */
-  int32_t schedule;    /* e2e_vi_opts.schedule of the batched launches (0 = autotuned) */
+  int32_t schedule;    /* e2e_vi_opts.schedule of the batched launches (0 = rule-based, no timing runs) */
 } e2e_server_opts;
 
 typedef struct {

@@ -72,6 +72,14 @@ def test_every_batch_schedule(models, graph):
             _check(models, vs, ps)
 
 
+def test_rule_based_schedule(models):
+    ms = [m for _, _, m, _, _ in models]
+    for sch in (0x400, 0x400 | 0x200, 0x400 | 4):
+        vs, ps = _outputs(models)
+        api.solve_batch(ms, vs, ps, schedule=sch)
+        _check(models, vs, ps)
+
+
 def test_batch_of_one_and_order_independence(models):
     import torch
     name, prob, m, V, pi = models[2]
