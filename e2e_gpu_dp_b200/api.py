@@ -103,7 +103,7 @@ class Model:
         sweep) or "jacobi" (reference semantics).  With ``value``/``policy`` CUDA
         tensors the results stay on the device; otherwise numpy arrays are returned.
         ``schedule``: the ``schedule`` word of e2e_vi_opts (0 = automatic; bits 0-3
-        warps per chunk, bit 8 set: bits 4-6 sweep tuning)."""
+        warps per chunk, bit 8 set: bits 4-7 sweep tuning)."""
         inf = self.info()
         ns = inf["ns"]
         o = _lib.ViOpts(1 if method == "layered" else 0, threshold, max_iter, timeout_s,

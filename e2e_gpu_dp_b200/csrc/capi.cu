@@ -734,14 +734,14 @@ e2e_status solve_on_device(const e2e_model* m, const e2e_vi_opts& o, float* dV, 
                            e2e_vi_stats* stats, cudaStream_t st) {
   const int64_t ns = m->ns;
   const int gsel = o.schedule & 15;
-  if ((o.schedule & ~0x17f) || (gsel != 0 && gsel != 1 && gsel != 2 && gsel != 4 && gsel != 8))
+  if ((o.schedule & ~0x1ff) || (gsel != 0 && gsel != 1 && gsel != 2 && gsel != 4 && gsel != 8))
     return fail(E2E_ERR_INVALID,
-                "schedule: bits 0-3 warps per chunk (0, 1, 2, 4, 8), bits 4-6 sweep tuning, bit 8 tuning given");
+                "schedule: bits 0-3 warps per chunk (0, 1, 2, 4, 8), bits 4-7 sweep tuning, bit 8 tuning given");
   // sweep tuning: given, or the defaults measured on B200 (layered: look-ahead
   // kernel, next layer's chunks prefetched into L2; Jacobi: lean kernel)
   const bool tune_given = (o.schedule & 0x100) != 0;
-  const int tune_layered = tune_given ? (o.schedule >> 4) & 7 : VI_TUNE_PF_NEXT;
-  const int tune_jacobi = tune_given ? (o.schedule >> 4) & 7 : VI_TUNE_LEAN;
+  const int tune_layered = tune_given ? (o.schedule >> 4) & 15 : VI_TUNE_PF_NEXT;
+  const int tune_jacobi = tune_given ? (o.schedule >> 4) & 15 : VI_TUNE_LEAN;
   double pack_ms = 0.0;
   {
     e2e_status ps = ensure_pack(m, &pack_ms, st);
@@ -786,7 +786,7 @@ e2e_status solve_on_device(const e2e_model* m, const e2e_vi_opts& o, float* dV, 
     int32_t* pi2 = nullptr;
     CK(dalloc((void**)&pi2, sizeof(int32_t) * (size_t)ns, st));
     scratch.add(pi2);
-    CK(launch_vi_chunks(P, 0, P.nchunks, dV, W, pi2, resid, st, tune_jacobi));
+    CK(launch_vi_chunks(P, 0, P.nchunks, dV, W, pi2, resid, st, tune_jacobi, syncw + 1));
     unsigned long long h = 0;
     CK(cudaMemcpyAsync(&h, resid, sizeof(h), cudaMemcpyDeviceToHost, st));
     CK(cudaEventRecord(e1, st));
@@ -801,7 +801,7 @@ e2e_status solve_on_device(const e2e_model* m, const e2e_vi_opts& o, float* dV, 
     while (!done) {
       if (iters >= max_iter) break;
       ++iters;
-      CK(launch_vi_chunks(P, 0, P.nchunks, a, b, dpi, resid + iters, st, tune_jacobi));
+      CK(launch_vi_chunks(P, 0, P.nchunks, a, b, dpi, resid + iters, st, tune_jacobi, syncw + 1));
       unsigned long long h = 0;
       CK(cudaMemcpyAsync(&h, resid + iters, sizeof(h), cudaMemcpyDeviceToHost, st));
       CK(cudaStreamSynchronize(st));
@@ -833,7 +833,7 @@ e2e_status solve_on_device(const e2e_model* m, const e2e_vi_opts& o, float* dV, 
     unsigned int herr = 0;
     CK(cudaMemcpyAsync(&herr, syncw + 1, sizeof(herr), cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
-    if (herr) return fail(E2E_ERR_DEVICE, "a bounded grid barrier of the layered sweep gave up");
+    if (herr) return fail(E2E_ERR_DEVICE, "a bounded device-side wait of the sweep gave up");
   }
   float ms = 0.f, ms_pass = 0.f;
   CK(cudaEventElapsedTime(&ms, e0, e1));

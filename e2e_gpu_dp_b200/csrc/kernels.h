@@ -126,12 +126,14 @@ void free_pack(PackStore* p);
 int64_t pack_sweep_bytes(const ViPack& P);
 // tune bits of the sweeps: L2 bulk prefetch of the chunk a warp takes next
 // (the next layer's, when layered) and/or of the chunk it starts; the lean
-// kernel (no entry look-ahead, 8 CTAs per SM) instead of the look-ahead one
-enum : int { VI_TUNE_PF_NEXT = 1, VI_TUNE_PF_CURRENT = 2, VI_TUNE_LEAN = 4 };
+// kernel (no entry look-ahead, 8 CTAs per SM) instead of the look-ahead one;
+// for the Jacobi sweep of the packed layout, the TMA-staged kernel
+enum : int { VI_TUNE_PF_NEXT = 1, VI_TUNE_PF_CURRENT = 2, VI_TUNE_LEAN = 4, VI_TUNE_TMA = 8 };
 // One Jacobi sweep over chunks [c_begin, c_end).
+// err: device word for bounded-wait failures (needed by the TMA-staged kernel)
 cudaError_t launch_vi_chunks(const ViPack& P, int64_t c_begin, int64_t c_end, const float* Vin,
                              float* Vout, int32_t* pi, unsigned long long* resid, cudaStream_t st,
-                             int tune);
+                             int tune, unsigned int* err = nullptr);
 // The whole layered schedule in one cooperative launch, in place on V.
 // sync: two zeroed words (barrier count, error bits); groups: warps per chunk
 // (1, 2, 4, 8; 0 picks one).

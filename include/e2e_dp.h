@@ -141,9 +141,10 @@ typedef struct {
   double timeout_s;      /* host wall-clock limit, 0 = none */
   int32_t fp64_check;    /* 1: FP64 backward solve on the device, report the error of the FP32 values */
   int32_t schedule;      /* 0 = automatic.  Bits 0-3: warps sharing a 32-state chunk in the layered
-                            sweep (0 = auto, 1, 2, 4, 8).  Bit 8 set: bits 4-6 give the sweep
+                            sweep (0 = auto, 1, 2, 4, 8).  Bit 8 set: bits 4-7 give the sweep
                             tuning (4: L2 prefetch of the chunk a warp takes next, 5: of the chunk
-                            it starts, 6: lean kernel without entry look-ahead). */
+                            it starts, 6: lean kernel without entry look-ahead, 7: Jacobi sweeps
+                            staged through shared memory by TMA bulk copies). */
 } e2e_vi_opts;
 
 typedef struct {
