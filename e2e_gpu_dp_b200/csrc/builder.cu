@@ -239,6 +239,10 @@ __global__ void __launch_bounds__(1024) k_build_tiles(BuildArgs A) {
   const float xsn = P.xsn, ys0 = P.ys0, dt = P.dt, r_out = P.r_out;
   const int kx = 0x4B400000 + wj0;  // float bits of 1.5*2^23 plus the window origin:
   const int ky = 0x4B400000 + wi0;  // round_half_up_index then gives window-local indices
+  // the same constants as (x, y) pairs for the packed float2 instructions
+  const float2 FF = make_float2(F, F), csn = make_float2(cs, sn), dt2 = make_float2(dt, dt);
+  const float2 xy1 = make_float2(x1, y1);
+  const float2 sgn = make_float2(1.0f, -1.0f), org = make_float2(-xs0, ysn);
 
   // Full reference expression for one sample (rare): reward, counts, dense
   // switch and drop accounting.
@@ -299,12 +303,14 @@ __global__ void __launch_bounds__(1024) k_build_tiles(BuildArgs A) {
     for (int q = a; q < clen; q += per) {
       if (cvalid) {
         const float* y = A.F.Y + ((int64_t)T * P.nrzns + base + q) * nm;
-        float sum_x = 0;
-        float sum_y = 0;
-        for (int k = 0; k < nm; k++) sum_x += modes[k * 32 + cl] * __ldg(y + k);
-        for (int k = 0; k < nm; k++) sum_y += modes[(nm + k) * 32 + cl] * __ldg(y + k);
-        // extract_velocity, src/build_model.cu:389-401: mean + sum over modes
-        myvel[q] = make_float2(u1 + sum_x, v1 + sum_y);
+        // extract_velocity, src/build_model.cu:389-401: mean + sum over modes,
+        // both sums as one chain of packed fused multiply-adds
+        float2 sum = make_float2(0.f, 0.f);
+        for (int k = 0; k < nm; k++) {
+          const float yk = __ldg(y + k);
+          sum = __ffma2_rn(make_float2(modes[k * 32 + cl], modes[(nm + k) * 32 + cl]), make_float2(yk, yk), sum);
+        }
+        myvel[q] = make_float2(u1 + sum.x, v1 + sum.y);
       }
     }
     __syncwarp();
@@ -316,14 +322,11 @@ __global__ void __launch_bounds__(1024) k_build_tiles(BuildArgs A) {
 #pragma unroll 4
         for (int q = 0; q < clen; ++q) {
           const float2 vv = myvel[q];
-          float vnetx = F * cs + vv.x;  // move(), src/build_model.cu:284-289
-          float vnety = F * sn + vv.y;
-          float xnew = x1 + (vnetx * dt);
-          float ynew = y1 + (vnety * dt);
-          const float ax = fminf(fmaxf(xnew - xs0, 0.0f), axmax);
-          const float ay = fminf(fmaxf(-(ynew - ysn), 0.0f), aymax);
-          const int lj = round_half_up_index(ax, kx);
-          const int li = round_half_up_index(ay, ky);
+          const float2 xy = advect2(FF, csn, vv, dt2, xy1);  // move(), src/build_model.cu:284-289
+          const float2 d = __ffma2_rn(xy, sgn, org);           // (xnew - xs0, -(ynew - ysn))
+          const float2 ad = make_float2(fminf(fmaxf(d.x, 0.0f), axmax), fminf(fmaxf(d.y, 0.0f), aymax));
+          int lj, li;
+          round_half_up_index2(ad, kx, ky, lj, li);
           const bool inw = (unsigned)(li | lj) < (unsigned)kWin;
           const int b = inw ? (li << 3) + lj : 0;
           uint16_t* wp = wcol + (b << log2S);
@@ -340,17 +343,14 @@ __global__ void __launch_bounds__(1024) k_build_tiles(BuildArgs A) {
         const uint64_t m_slow = masks[MASK_SLOW * nthr + tid];
         for (int q = 0; q < clen; ++q) {
           const float2 vv = myvel[q];
-          float vnetx = F * cs + vv.x;
-          float vnety = F * sn + vv.y;
-          float xnew = x1 + (vnetx * dt);
-          float ynew = y1 + (vnety * dt);
+          const float2 xy = advect2(FF, csn, vv, dt2, xy1);
+          const float xnew = xy.x, ynew = xy.y;
           const int kcl = ((xnew > xsn) || (xnew < xs0) ? 1 : 0) + ((ynew > ysn) || (ynew < ys0) ? 1 : 0);
           int li, lj;
           if (UNIT) {
-            const float ax = fminf(fmaxf(xnew - xs0, 0.0f), axmax);
-            const float ay = fminf(fmaxf(-(ynew - ysn), 0.0f), aymax);
-            lj = round_half_up_index(ax, kx);
-            li = round_half_up_index(ay, ky);
+            const float2 d = __ffma2_rn(xy, sgn, org);
+            const float2 ad = make_float2(fminf(fmaxf(d.x, 0.0f), axmax), fminf(fmaxf(d.y, 0.0f), aymax));
+            round_half_up_index2(ad, kx, ky, lj, li);
           } else {
             int i2, j2;
             land<UNIT>(P, F, cs, sn, vv.x, vv.y, x1, y1, i2, j2);

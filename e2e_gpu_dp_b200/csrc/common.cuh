@@ -164,6 +164,22 @@ __device__ __forceinline__ int32_t round_half_up_index(float a, int32_t bias) {
   return __float_as_int(t) - bias;            // bias = bits of 1.5*2^23 (+ window origin)
 }
 
+// advect() on (x, y) pairs with the packed float2 instructions of sm_100:
+// each component is the same fused multiply-add, rounded the same way.
+__device__ __forceinline__ float2 advect2(float2 FF, float2 csn, float2 v, float2 dt2, float2 xy) {
+  const float2 vnet = __ffma2_rn(FF, csn, v);  // (F*cs + vx, F*sn + vy)
+  return __ffma2_rn(vnet, dt2, xy);            // (x + vnetx*dt, y + vnety*dt)
+}
+
+// round_half_up_index() of both coordinates with the packed adds.
+__device__ __forceinline__ void round_half_up_index2(float2 a, int32_t bias_x, int32_t bias_y,
+                                                     int32_t& jx, int32_t& iy) {
+  const float2 w = __fadd2_rd(a, make_float2(0.5f, 0.5f));
+  const float2 t = __fadd2_rd(w, make_float2(12582912.0f, 12582912.0f));
+  jx = __float_as_int(t.x) - bias_x;
+  iy = __float_as_int(t.y) - bias_y;
+}
+
 __device__ __forceinline__ void land_unit(const DevProblem& P, float F, float cs, float sn,
                                           float vx, float vy, float x, float y, int& i2, int& j2) {
   float xnew, ynew;
