@@ -33,6 +33,7 @@ namespace e2e {
 
 static constexpr int kWin = 8;        // fast window side: bin = li * 8 + lj
 static constexpr int kWinBins = kWin * kWin;
+static constexpr int kMissBin = kWinBins;  // extra counter row: plain-loop samples that left the window
 static constexpr int kNb = 6;         // per-cell obstacle bitmap radius (13 x 13 around S1)
 static constexpr int kNbSide = 2 * kNb + 1;
 static constexpr int kNbBits = kNbSide * kNbSide;
@@ -102,15 +103,15 @@ __global__ void __launch_bounds__(1024) k_build_tiles(BuildArgs A) {
   const int nm = P.nm;
   const int log2S = counter_log2_stride(nthr);
 
-  float* modes = reinterpret_cast<float*>(smem);                           // 2*nm x 32
-  float2* velw = reinterpret_cast<float2*>(modes + 2 * nm * 32);           // 32 x kVelStride
+  float2* modes = reinterpret_cast<float2*>(smem);                         // nm x 32: (ui, vi)
+  float2* velw = modes + nm * 32;                                          // 32 x kVelStride
   uint64_t* masks = reinterpret_cast<uint64_t*>(velw + 32 * kVelStride);   // MASK_COUNT x nthr
-  uint16_t* win = reinterpret_cast<uint16_t*>(masks + MASK_COUNT * nthr);  // 64 x S
+  uint16_t* win = reinterpret_cast<uint16_t*>(masks + MASK_COUNT * nthr);  // 65 x S: bins, miss bin
   __shared__ uint32_t obsmap[32][kNbWords];
   __shared__ float tab[32][8];
   uint16_t* const wcol = win + counter_col(warp, lane);
 
-  // ---- stage the modes of the tile's cells (ui then vi) -------------------
+  // ---- stage the modes of the tile's cells as (ui_k, vi_k) pairs ---------
   for (int idx = tid; idx < 2 * nm * 32; idx += nthr) {
     int k2 = idx >> 5, l = idx & 31;
     int64_t c = c0 + l;
@@ -119,7 +120,8 @@ __global__ void __launch_bounds__(1024) k_build_tiles(BuildArgs A) {
       val = (k2 < nm) ? __ldg(A.F.ui + ((int64_t)T * nm + k2) * nc + c)
                       : __ldg(A.F.vi + ((int64_t)T * nm + (k2 - nm)) * nc + c);
     }
-    modes[idx] = val;
+    const int k = k2 < nm ? k2 : k2 - nm;
+    reinterpret_cast<float*>(modes)[2 * (k * 32 + l) + (k2 < nm ? 0 : 1)] = val;
   }
   for (int idx = tid; idx < 32 * kNbWords; idx += nthr) obsmap[idx / kNbWords][idx % kNbWords] = 0u;
   const bool late = T > P.nt - 20;
@@ -181,7 +183,7 @@ __global__ void __launch_bounds__(1024) k_build_tiles(BuildArgs A) {
     r_fixed = P.r_out;
   }
   __syncthreads();  // obsmap complete
-  for (int b = 0; b < kWinBins; ++b) wcol[b << log2S] = 0;
+  for (int b = 0; b <= kMissBin; ++b) wcol[b << log2S] = 0;
   int wi0 = 0, wj0 = 0;
   uint64_t ovr = 0, inwin = 0, edge = 0, term = 0, slow = 0;
   if (mode == MODE_WINDOW) {
@@ -244,6 +246,21 @@ __global__ void __launch_bounds__(1024) k_build_tiles(BuildArgs A) {
   const float2 xy1 = make_float2(x1, y1);
   const float2 sgn = make_float2(1.0f, -1.0f), org = make_float2(-xs0, ysn);
 
+  // In-window rewards of a plain row, from its counters: such a sample's
+  // reward is r_plain, or r_outbound in an obstacle-overridden bin, so the
+  // row's sum gains count x reward per bin kind instead of one addition per
+  // sample (the reference adds them with float atomics in no fixed order).
+  auto fold_window = [&]() {
+    uint32_t n_pl = 0, n_ovr = 0;
+    for (int wl = 0; wl < kWinBins; ++wl) {
+      const uint32_t w = wcol[wl << log2S];
+      if (w & kOvrFlag) n_ovr += w & kCountMask;
+      else n_pl += w;
+    }
+    sumR += (float)n_pl * r_plain;
+    sumR += (float)n_ovr * r_out;
+  };
+
   // Full reference expression for one sample (rare): reward, counts, dense
   // switch and drop accounting.
   auto full_sample = [&](float vx, float vy, int i2, int j2) -> float {
@@ -271,6 +288,7 @@ __global__ void __launch_bounds__(1024) k_build_tiles(BuildArgs A) {
     if (di >= 0 && di < P.m && dj >= 0 && dj < P.m) {
       if (mode == MODE_WINDOW) {
         // switch this row to a dense m*m histogram from the pool
+        if (plain_warp) fold_window();  // the window's samples are final
         unsigned long long slot = atomicAdd(A.counters + CTR_POOL, 1ull);
         atomicAdd(A.counters + CTR_OVERFLOW_ROWS, 1ull);
         if (slot < (unsigned long long)A.pool_units) {
@@ -308,7 +326,7 @@ __global__ void __launch_bounds__(1024) k_build_tiles(BuildArgs A) {
         float2 sum = make_float2(0.f, 0.f);
         for (int k = 0; k < nm; k++) {
           const float yk = __ldg(y + k);
-          sum = __ffma2_rn(make_float2(modes[k * 32 + cl], modes[(nm + k) * 32 + cl]), make_float2(yk, yk), sum);
+          sum = __ffma2_rn(modes[k * 32 + cl], make_float2(yk, yk), sum);
         }
         myvel[q] = make_float2(u1 + sum.x, v1 + sum.y);
       }
@@ -319,24 +337,28 @@ __global__ void __launch_bounds__(1024) k_build_tiles(BuildArgs A) {
     } else if (mode == MODE_WINDOW) {
       int n_out = 0;
       if (plain_warp) {
+        // counts only: the rewards are folded from the counters at the end, a
+        // sample that leaves the window counts in the miss bin
 #pragma unroll 4
         for (int q = 0; q < clen; ++q) {
           const float2 vv = myvel[q];
           const float2 xy = advect2(FF, csn, vv, dt2, xy1);  // move(), src/build_model.cu:284-289
-          const float2 d = __ffma2_rn(xy, sgn, org);           // (xnew - xs0, -(ynew - ysn))
-          const float2 ad = make_float2(fminf(fmaxf(d.x, 0.0f), axmax), fminf(fmaxf(d.y, 0.0f), aymax));
+          // (xnew - xs0, -(ynew - ysn)) without the domain clamps: a plain
+          // row's window holds no edge cell, so a sample the clamps would move
+          // lands outside the window either way (unclamped its index is below 0
+          // or above g-1; a NaN or a value beyond 2^22 gives bits far from the
+          // bias) and is taken again by the rescan below
+          const float2 d = __ffma2_rn(xy, sgn, org);
           int lj, li;
-          round_half_up_index2(ad, kx, ky, lj, li);
+          round_half_up_index2(d, kx, ky, lj, li);
           const bool inw = (unsigned)(li | lj) < (unsigned)kWin;
-          const int b = inw ? (li << 3) + lj : 0;
+          const int b = inw ? (li << 3) + lj : kMissBin;
           uint16_t* wp = wcol + (b << log2S);
-          const uint32_t w = *wp;
-          const float r = (w & kOvrFlag) ? r_out : r_plain;
-          *wp = (uint16_t)(inw ? w + 1 : w);  // branch-free: a miss writes bin 0 back
-          const float s2 = sumR + r;
-          sumR = inw ? s2 : sumR;
-          n_out += inw ? 0 : 1;
+          *wp = (uint16_t)(*wp + 1);
         }
+        uint16_t* mp = wcol + (kMissBin << log2S);
+        n_out = *mp;
+        if (n_out) *mp = 0;
       } else {
         const uint64_t m_edge = masks[MASK_EDGE * nthr + tid];
         const uint64_t m_term = masks[MASK_TERM * nthr + tid];
@@ -381,7 +403,8 @@ __global__ void __launch_bounds__(1024) k_build_tiles(BuildArgs A) {
           const int li = i2 - wi0, lj = j2 - wj0;
           const bool inw = (unsigned)(li | lj) < (unsigned)kWin;
           if (inw && !bit64(m_slow, (li << 3) + lj)) continue;
-          sumR += full_sample(vv.x, vv.y, i2, j2);
+          const float r = full_sample(vv.x, vv.y, i2, j2);
+          sumR += r;
         }
       }
     } else if (mode == MODE_DENSE) {
@@ -389,10 +412,12 @@ __global__ void __launch_bounds__(1024) k_build_tiles(BuildArgs A) {
         const float2 vv = myvel[q];
         int i2, j2;
         land<UNIT>(P, F, cs, sn, vv.x, vv.y, x1, y1, i2, j2);
-        sumR += full_sample(vv.x, vv.y, i2, j2);
+        const float r = full_sample(vv.x, vv.y, i2, j2);
+        sumR += r;
       }
     }
   }
+  if (plain_warp && mode == MODE_WINDOW) fold_window();
   if (n_drop) atomicAdd(A.counters + CTR_DROPPED, (unsigned long long)n_drop);
   if (n_misbin) atomicAdd(A.counters + CTR_MISBIN, (unsigned long long)n_misbin);
   if (mode == MODE_LOST) atomicOr(reinterpret_cast<unsigned int*>(A.counters + CTR_FLAGS), FLAG_POOL_EXHAUSTED);
@@ -586,7 +611,7 @@ size_t build_smem_bytes(int na, int nm, int rc) {
   const int nthr = 32 << build_lanes_log2(na);
   return (size_t)2 * nm * 32 * sizeof(float) + (size_t)32 * kVelStride * sizeof(float2) +
          (size_t)MASK_COUNT * nthr * sizeof(uint64_t) +
-         (size_t)kWinBins * ((size_t)1 << counter_log2_stride(nthr)) * sizeof(uint16_t);
+         (size_t)(kWinBins + 1) * ((size_t)1 << counter_log2_stride(nthr)) * sizeof(uint16_t);
 }
 
 template <typename CntT, bool UNIT>
