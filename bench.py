@@ -86,6 +86,7 @@ class Clocks:
         self.samples.append((float(sm), float(smax), int(reasons)))
 
     def __enter__(self):
+        """NVML set-up (before the warm-up steps); sampling starts at begin()."""
         try:
             import pynvml as nv
 
@@ -98,9 +99,16 @@ class Clocks:
             self.samples.clear()
             self._nv, self._h = nv, h
             self.thread = True       # NVML mode
-            return self
         except Exception:
             self.thread = None
+        return self
+
+    def begin(self):
+        """Start of the timed region: NVML samples are taken by tick(); without
+        NVML an nvidia-smi sampler runs until exit."""
+        if self.thread is not None:
+            self.samples.clear()
+            return
         try:
             sel = ["-i", self._uuid()]
         except Exception:
@@ -116,7 +124,6 @@ class Clocks:
                 time.sleep(0.05)   # its first sample is taken before timing starts
         except Exception:
             self.proc = None
-        return self
 
     def tick(self):
         """One sample (NVML mode), called between steps."""
@@ -267,29 +274,28 @@ def run_ours(args, ws, rank, local):
             record.append((m.info(), st, (round((t1 - t0) * 1e3, 1), round((t2 - t1) * 1e3, 1))))
         m.free()
 
-    for _ in range(args.warmup):
-        step()
-    torch.cuda.synchronize()
-    _barrier(ws)
     recs = []
-    e0 = torch.cuda.Event(enable_timing=True)
-    e1 = torch.cuda.Event(enable_timing=True)
-    marks = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps + 1)]
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
     with Clocks(local) as clk:
+        for _ in range(args.warmup):
+            step()
         torch.cuda.synchronize()
-        e0.record(stream)
+        _barrier(ws)
+        clk.begin()
+        torch.cuda.synchronize()
+        # each step between its own events: the clock sample taken between two
+        # steps (host only, GPU idle) is not part of either
         for k in range(args.steps):
+            starts[k].record(stream)
             step(recs)
-            marks[k + 1].record(stream)
+            ends[k].record(stream)
             torch.cuda.synchronize()
             clk.tick()
-        e1.record(stream)
         torch.cuda.synchronize()
     _barrier(ws)
-    ms = e0.elapsed_time(e1) / args.steps
-    step_ms = [round(e0.elapsed_time(marks[1]), 2)] + [round(marks[k].elapsed_time(marks[k + 1]), 2)
-                                                        for k in range(1, args.steps)]
-    ms = _max_over_ranks(ms, ws)
+    step_ms = [round(starts[k].elapsed_time(ends[k]), 2) for k in range(args.steps)]
+    ms = _max_over_ranks(sum(starts[k].elapsed_time(ends[k]) for k in range(args.steps)) / args.steps, ws)
     clocks = clk.summary()
 
     info = recs[-1][0]
@@ -365,6 +371,25 @@ def run_ours(args, ws, rank, local):
                         "outcome_agreement_on_sample": same,
                         "speedup_vs_cpu": round(cpu_s / max(ro2["stats"]["seconds"], 1e-9), 1)})
 
+    # fused build+backup (e2e_build_solve): each layer backed up as it is built,
+    # no model stored; compared with the build + layered solve just above
+    Vf = torch.empty_like(V)
+    pif = torch.empty_like(pi)
+    api.build_solve(prob, dev, value=Vf, policy=pif, stream=stream)
+    fused_ms = []
+    for _ in range(3):
+        g0 = torch.cuda.Event(enable_timing=True)
+        g1 = torch.cuda.Event(enable_timing=True)
+        g0.record(stream)
+        _, _, fst = api.build_solve(prob, dev, value=Vf, policy=pif, stream=stream)
+        g1.record(stream)
+        torch.cuda.synchronize()
+        fused_ms.append(g0.elapsed_time(g1))
+    fused = {"api": "e2e_build_solve", "ms": [round(x, 2) for x in fused_ms],
+             "kernel_ms": round(fst["seconds"] * 1e3, 2), "launches": fst["launches"], "nnz": fst["nnz"],
+             "identical_to_build_then_solve": bool(torch.equal(Vf, V) and torch.equal(pif, pi)),
+             "speedup_vs_step": round(ms / statistics.median(fused_ms), 3)}
+
     cb = 2 if info["count_type"] == 0 else 4
     k1_bytes = algorithmic_build_bytes(prob, info["nnz"], cb)
     k1_gbs = k1_bytes / (k1_ms * 1e-3) / 1e9
@@ -420,6 +445,7 @@ def run_ours(args, ws, rank, local):
                "layered_pass_seconds": round(lst["sweep_seconds"], 6),
                "fp64_max_rel_err": lst["fp64_max_rel_err"]},
         "rollout": rollout,
+        "fused_build_solve": fused,
         "clocks": clocks,
     }
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
@@ -702,9 +728,11 @@ def run_reference(args, ws, rank, local):
             run_ref.run("t_time", os.path.join(work, "warm"), keep_model=False)
         runs = []
         with Clocks(local) as clk:
+            clk.begin()
             for _ in range(args.steps):
                 runs.append(run_ref.run(WORKLOAD, os.path.join(work, "c2"), prob=prob, fields=fields,
                                         keep_model=False))
+                clk.tick()
         clocks = clk.summary()
     finally:
         subprocess.run(["rm", "-rf", work])

@@ -13,6 +13,7 @@ _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "libe2edp.so")
 
 E2E_OK = 0
+E2E_ERR_INVALID = 1
 E2E_HOST, E2E_DEVICE = 0, 1
 E2E_COUNT_U16, E2E_COUNT_U32, E2E_VALUE_F32, E2E_COUNT_AUTO = 0, 1, 2, -1
 
@@ -115,6 +116,12 @@ class RolloutStats(C.Structure):
                 ("mean_net_energy", C.c_double), ("seconds", C.c_double)]
 
 
+class FusedStats(C.Structure):
+    _fields_ = [("seconds", C.c_double), ("n_rows", C.c_int64), ("nnz", C.c_int64), ("dropped", C.c_uint64),
+                ("misbinned", C.c_uint64), ("overflow_rows", C.c_uint64), ("launches", C.c_int32),
+                ("reserved", C.c_int32), ("h2d_bytes", C.c_int64)]
+
+
 # every exported symbol of include/e2e_dp.h with its signature
 SIGNATURES = {
     "e2e_abi_version": (C.c_int, []),
@@ -144,6 +151,8 @@ SIGNATURES = {
     "e2e_rollout": (C.c_int, [C.POINTER(Problem), C.POINTER(Fields), C.c_int, C.c_void_p, C.c_int,
                               C.POINTER(RolloutOpts), C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                               C.POINTER(RolloutStats), C.c_void_p]),
+    "e2e_build_solve": (C.c_int, [C.POINTER(Problem), C.POINTER(Fields), C.c_int, C.c_void_p, C.c_void_p,
+                                  C.c_int, C.POINTER(FusedStats), C.c_void_p]),
     "e2e_server_create": (C.c_int, [C.POINTER(ServerOpts), C.POINTER(C.c_void_p)]),
     "e2e_server_add_field": (C.c_int, [C.c_void_p, C.POINTER(Problem), C.POINTER(Fields), C.c_int,
                                        C.POINTER(C.c_int32)]),

@@ -272,6 +272,31 @@ class Server:
             pass
 
 
+def build_solve(prob: Problem, fields: Dict, value=None, policy=None, stream=None):
+    """Build and solve in one backward pass without storing the model
+    (e2e_build_solve): layer t's rows are backed up as soon as they are built.
+    ``value`` / ``policy``: optional CUDA tensors of ns float32 / int32 to fill;
+    otherwise host numpy arrays are returned.  Returns (V, policy, stats)."""
+    where, f, keep = _fields_ptrs(fields)
+    st = _lib.FusedStats()
+    cp = c_problem(prob)
+    if value is not None or policy is not None:
+        if value is None or policy is None or not (_is_device(value) and _is_device(policy)):
+            raise ValueError("pass both value and policy as CUDA tensors, or neither")
+        if value.numel() != prob.ns or policy.numel() != prob.ns:
+            raise ValueError("value and policy need ns entries")
+        V, pi = value, policy
+        out_where, vptr, pptr = _lib.E2E_DEVICE, value.data_ptr(), policy.data_ptr()
+    else:
+        V = np.empty(prob.ns, np.float32)
+        pi = np.empty(prob.ns, np.int32)
+        out_where, vptr, pptr = _lib.E2E_HOST, V.ctypes.data, pi.ctypes.data
+    check(lib().e2e_build_solve(C.byref(cp), C.byref(f), where, pptr, vptr, out_where, C.byref(st),
+                                _stream_ptr(stream)))
+    del keep
+    return V, pi, {k: getattr(st, k) for k, _ in _lib.FusedStats._fields_}
+
+
 def rollout(prob: Problem, fields: Dict, policy, start, n_rzns: int = 0, stream=None) -> Dict:
     """Follow ``policy`` (ns int32, numpy or CUDA tensor) from ``start`` (i, j)
     for each realisation (e2e_rollout).  Returns per-realisation arrays and

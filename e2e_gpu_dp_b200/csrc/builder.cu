@@ -61,6 +61,70 @@ __host__ __device__ __forceinline__ int counter_log2_stride(int nthr) {
   return l;
 }
 
+// Backup of the lane's row (cell, action a) of layer T from its counters:
+// Q = R + (sum over entries in column order of fma(count, V[col], acc)) / nrzns
+// with R = sumR / nrzns, the arithmetic of the value-iteration sweeps
+// (solver_do_backup, src/spvi_2.cu:174-260) on the row the staging path would
+// emit; then the first maximum over the cell's action lanes (select_best_action,
+// src/spvi_2.cu:93-122: strict '>', NaN never taken, values at or below -1e6
+// give -1e6 / -1) and one write of V and the policy per cell.  Entries are
+// counted into CTR_STAGE (the model's nnz) per warp.
+__device__ __forceinline__ void fused_backup(const BuildArgs& A, int T, int64_t cell, bool valid, bool cvalid,
+                                             int a, int lane, int lanes_log2, int mode, float sumR,
+                                             const uint16_t* wcol, int log2S, int wi0, int wj0, int i1,
+                                             int j1, const uint32_t* dense) {
+  const DevProblem& P = A.P;
+  const int g = P.g;
+  const int64_t nc = (int64_t)g * g;
+  // values of layer T+1 are complete once the previous launch has completed
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+  const float* Vn = A.V + (int64_t)(T + 1) * nc;
+  float acc = 0.f;
+  int nnz = 0;
+  if (valid) {
+    if (mode == MODE_FIXED) {
+      acc = fmaf((float)P.nrzns, Vn[cell], acc);
+      nnz = 1;
+    } else if (mode == MODE_WINDOW) {
+      for (int wl = 0; wl < kWinBins; ++wl) {
+        const uint32_t c = wcol[wl << log2S] & kCountMask;
+        if (c) {
+          acc = fmaf((float)c, Vn[(int64_t)(wi0 + wl / kWin) * g + wj0 + wl % kWin], acc);
+          ++nnz;
+        }
+      }
+    } else if (mode == MODE_DENSE) {
+      for (int b = 0; b < P.m * P.m; ++b) {
+        const uint32_t c = dense[b];
+        if (c) {
+          acc = fmaf((float)c, Vn[(int64_t)(b / P.m + i1 - P.del) * g + b % P.m + j1 - P.del], acc);
+          ++nnz;
+        }
+      }
+    }
+  }
+  const float R = sumR / P.nrzns;  // compute_mean, src/build_model.cu:567
+  float q = R + acc / (float)P.nrzns;
+  if (!valid || mode == MODE_LOST || isnan(q)) q = -INFINITY;
+  int ba = a;
+  const int per = 1 << lanes_log2;
+  for (int o = per >> 1; o > 0; o >>= 1) {
+    const float oq = __shfl_xor_sync(0xffffffffu, q, o);
+    const int oa = __shfl_xor_sync(0xffffffffu, ba, o);
+    if (oq > q || (oq == q && oa < ba)) {
+      q = oq;
+      ba = oa;
+    }
+  }
+  for (int o = 16; o > 0; o >>= 1) nnz += __shfl_xor_sync(0xffffffffu, nnz, o);
+  if (lane == 0 && nnz) atomicAdd(A.counters + CTR_STAGE, (unsigned long long)nnz);
+  if (cvalid && a == 0) {
+    const bool ok = q > -1e6f;
+    A.V[(int64_t)T * nc + cell] = ok ? q : -1e6f;
+    A.pi[(int64_t)T * nc + cell] = ok ? ba : -1;
+  }
+}
+
 // K1.  Template: CntT = staged count type; UNIT = unit cell spacing.
 //
 // A CTA owns 32 consecutive cells of one layer and all their actions.  Warp w
@@ -81,7 +145,11 @@ __host__ __device__ __forceinline__ int counter_log2_stride(int nthr) {
 // window (or lands on a slow bin) is only counted; a rescan of the chunk runs
 // the full reference expression for it afterwards, so its reward joins the
 // row's sum after the chunk's in-window rewards.
-template <typename CntT, bool UNIT>
+//
+// FUSED (one launch per layer, A.t0 = the layer): instead of staging the rows,
+// back them up at once against V of layer t+1 (finished by the previous launch
+// of the stream) and write V, policy of layer t; see fused_backup below.
+template <typename CntT, bool UNIT, bool FUSED>
 __global__ void __launch_bounds__(1024) k_build_tiles(BuildArgs A) {
   extern __shared__ __align__(16) unsigned char smem[];
   const DevProblem& P = A.P;
@@ -110,6 +178,11 @@ __global__ void __launch_bounds__(1024) k_build_tiles(BuildArgs A) {
   __shared__ uint32_t obsmap[32][kNbWords];
   __shared__ float tab[32][8];
   uint16_t* const wcol = win + counter_col(warp, lane);
+
+  // the next layer's launch may start its CTAs once every CTA of this one has
+  // started (programmatic dependent launch); it reads this layer's values only
+  // after griddepcontrol.wait, i.e. after this grid has completed
+  if (FUSED) asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
 
   // ---- stage the modes of the tile's cells as (ui_k, vi_k) pairs ---------
   for (int idx = tid; idx < 2 * nm * 32; idx += nthr) {
@@ -245,6 +318,7 @@ __global__ void __launch_bounds__(1024) k_build_tiles(BuildArgs A) {
   const float2 FF = make_float2(F, F), csn = make_float2(cs, sn), dt2 = make_float2(dt, dt);
   const float2 xy1 = make_float2(x1, y1);
   const float2 sgn = make_float2(1.0f, -1.0f), org = make_float2(-xs0, ysn);
+  const bool y_pairs = (nm % 2 == 0) && ((reinterpret_cast<uintptr_t>(A.F.Y) & 7) == 0);
 
   // In-window rewards of a plain row, from its counters: such a sample's
   // reward is r_plain, or r_outbound in an obstacle-overridden bin, so the
@@ -324,9 +398,19 @@ __global__ void __launch_bounds__(1024) k_build_tiles(BuildArgs A) {
         // extract_velocity, src/build_model.cu:389-401: mean + sum over modes,
         // both sums as one chain of packed fused multiply-adds
         float2 sum = make_float2(0.f, 0.f);
-        for (int k = 0; k < nm; k++) {
-          const float yk = __ldg(y + k);
-          sum = __ffma2_rn(modes[k * 32 + cl], make_float2(yk, yk), sum);
+        const float2* md = modes + cl;
+        if (y_pairs) {  // nm even, rows 8-byte aligned: coefficients two at a time
+#pragma unroll 2
+          for (int k = 0; k < nm; k += 2) {
+            const float2 yy = __ldg(reinterpret_cast<const float2*>(y + k));
+            sum = __ffma2_rn(md[k * 32], make_float2(yy.x, yy.x), sum);
+            sum = __ffma2_rn(md[(k + 1) * 32], make_float2(yy.y, yy.y), sum);
+          }
+        } else {
+          for (int k = 0; k < nm; k++) {
+            const float yk = __ldg(y + k);
+            sum = __ffma2_rn(md[k * 32], make_float2(yk, yk), sum);
+          }
         }
         myvel[q] = make_float2(u1 + sum.x, v1 + sum.y);
       }
@@ -339,7 +423,7 @@ __global__ void __launch_bounds__(1024) k_build_tiles(BuildArgs A) {
       if (plain_warp) {
         // counts only: the rewards are folded from the counters at the end, a
         // sample that leaves the window counts in the miss bin
-#pragma unroll 4
+#pragma unroll 8
         for (int q = 0; q < clen; ++q) {
           const float2 vv = myvel[q];
           const float2 xy = advect2(FF, csn, vv, dt2, xy1);  // move(), src/build_model.cu:284-289
@@ -421,6 +505,12 @@ __global__ void __launch_bounds__(1024) k_build_tiles(BuildArgs A) {
   if (n_drop) atomicAdd(A.counters + CTR_DROPPED, (unsigned long long)n_drop);
   if (n_misbin) atomicAdd(A.counters + CTR_MISBIN, (unsigned long long)n_misbin);
   if (mode == MODE_LOST) atomicOr(reinterpret_cast<unsigned int*>(A.counters + CTR_FLAGS), FLAG_POOL_EXHAUSTED);
+
+  if (FUSED) {
+    fused_backup(A, T, cell, valid, cvalid, a, lane, lanes_log2, mode, sumR, wcol, log2S, wi0, wj0, i1, j1,
+                 dense);
+    return;
+  }
 
   // ---- per-warp emission: row lengths, warp scan, one atomicAdd -----------
   int nnz = 0;
@@ -614,7 +704,7 @@ size_t build_smem_bytes(int na, int nm, int rc) {
          (size_t)(kWinBins + 1) * ((size_t)1 << counter_log2_stride(nthr)) * sizeof(uint16_t);
 }
 
-template <typename CntT, bool UNIT>
+template <typename CntT, bool UNIT, bool FUSED = false>
 static cudaError_t launch_one(const BuildArgs& A, int n_layers, cudaStream_t st) {
   dim3 grid((unsigned)A.tiles_per_layer, (unsigned)n_layers);
   dim3 block((unsigned)(32u << A.lanes_log2));
@@ -629,13 +719,29 @@ static cudaError_t launch_one(const BuildArgs& A, int n_layers, cudaStream_t st)
     if (e != cudaSuccess) return e;
     std::lock_guard<std::mutex> lk(mu);
     if (dev >= 0 && dev < 64 && (int)sm > cap_set[dev]) {
-      e = cudaFuncSetAttribute(k_build_tiles<CntT, UNIT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+      e = cudaFuncSetAttribute(k_build_tiles<CntT, UNIT, FUSED>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)sm);
       if (e != cudaSuccess) return e;
       cap_set[dev] = (int)sm;
     }
   }
-  k_build_tiles<CntT, UNIT><<<grid, block, sm, st>>>(A);
-  return cudaGetLastError();
+  if (!FUSED) {
+    k_build_tiles<CntT, UNIT, FUSED><<<grid, block, sm, st>>>(A);
+    return cudaGetLastError();
+  }
+  // programmatic dependent launch: this layer's CTAs start while the previous
+  // layer's last CTAs finish; griddepcontrol.wait orders the reads of its values
+  cudaLaunchConfig_t cfg{};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = sm;
+  cfg.stream = st;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, k_build_tiles<CntT, UNIT, FUSED>, A);
 }
 
 cudaError_t launch_build_tiles(const BuildArgs& A, int count_bits, int n_layers,
@@ -644,6 +750,12 @@ cudaError_t launch_build_tiles(const BuildArgs& A, int count_bits, int n_layers,
   if (count_bits == 16) return unit ? launch_one<uint16_t, true>(A, n_layers, st)
                                     : launch_one<uint16_t, false>(A, n_layers, st);
   return unit ? launch_one<uint32_t, true>(A, n_layers, st) : launch_one<uint32_t, false>(A, n_layers, st);
+}
+
+cudaError_t launch_build_fused(const BuildArgs& A, int layer, cudaStream_t st) {
+  BuildArgs B = A;
+  B.t0 = layer;
+  return A.P.unit_step != 0 ? launch_one<uint32_t, true, true>(B, 1, st) : launch_one<uint32_t, false, true>(B, 1, st);
 }
 
 cudaError_t launch_scan_tiles(const int32_t* tile_len, int64_t n_tiles, int64_t* canon,

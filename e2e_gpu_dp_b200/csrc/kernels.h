@@ -39,6 +39,8 @@ struct BuildArgs {
   float* sumR;                   // nullable: per-row reward sums (before the division)
   uint32_t* pool;                // pool_units x m*m dense histograms
   int64_t pool_units;
+  float* V;                      // fused build+backup: values (ns), layer t+1 read, layer t written
+  int32_t* pi;                   // fused build+backup: policy (ns)
 };
 
 struct AssembleArgs {
@@ -58,6 +60,9 @@ struct AssembleArgs {
 int build_lanes_log2(int na);
 size_t build_smem_bytes(int na, int nm, int rc);
 cudaError_t launch_build_tiles(const BuildArgs& A, int count_bits, int n_layers, cudaStream_t st);
+// One layer of the fused build+backup (uses A.V, A.pi, A.pool, A.counters;
+// no staging): launched for layers nt-2 down to 0 on one stream.
+cudaError_t launch_build_fused(const BuildArgs& A, int layer, cudaStream_t st);
 cudaError_t launch_scan_tiles(const int32_t* tile_len, int64_t n_tiles, int64_t* canon,
                               int64_t* total, int64_t* block_sums, cudaStream_t st);
 cudaError_t launch_assemble(const AssembleArgs& A, int count_bits, int index_bits,

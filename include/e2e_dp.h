@@ -343,6 +343,31 @@ e2e_status e2e_rollout(const e2e_problem* p, const e2e_fields* f, int fields_whe
                        int policy_where, const e2e_rollout_opts* opts, int8_t* success_out, int32_t* time_out,
                        float* energy_out, int32_t* final_out, e2e_rollout_stats* stats, void* stream);
 
+/* ---- build and solve in one backward pass ------------------------------------
+ * No counterpart in the reference, which writes the model between build_model
+ * and spvi_2.  Layers nt-2 down to 0: the rows of layer t are built exactly as
+ * by e2e_build_model and backed up at once against the finished values of
+ * layer t+1, so the transition model is never stored (device memory: the
+ * fields, V and policy).  Value and policy are bit-identical to
+ * e2e_build_model + e2e_spvi_solve with the layered method (whose fixed point
+ * is the Jacobi one); last layer: value 0, action 0.  policy_out / value_out:
+ * ns entries each in out_where memory (either may be NULL). */
+typedef struct {
+  double seconds;          /* device time of the per-layer launches (CUDA events) */
+  int64_t n_rows;          /* rows built and backed up */
+  int64_t nnz;             /* entries backed up (the model's nnz) */
+  uint64_t dropped;        /* as e2e_model_info */
+  uint64_t misbinned;
+  uint64_t overflow_rows;
+  int32_t launches;        /* kernel launches (nt - 1 per pass; a pass is re-run when rows needed more dense histograms) */
+  int32_t reserved;
+  int64_t h2d_bytes;       /* field bytes copied from host memory */
+} e2e_fused_stats;
+
+e2e_status e2e_build_solve(const e2e_problem* p, const e2e_fields* fields, int fields_where,
+                           int32_t* policy_out, float* value_out, int out_where,
+                           e2e_fused_stats* stats /* may be NULL */, void* stream);
+
 /* ---- solve without device allocation ----------------------------------------
  * No counterpart in the reference.  For callers that cannot allocate device
  * memory (a serving loop whose memory is fully reserved by its own pool, or code
