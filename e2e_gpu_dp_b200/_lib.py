@@ -122,6 +122,27 @@ class FusedStats(C.Structure):
                 ("reserved", C.c_int32), ("h2d_bytes", C.c_int64)]
 
 
+E2E_OBST_NONE, E2E_OBST_STATIC, E2E_OBST_DYNAMIC = 0, 1, 2
+
+
+class EnvParams(C.Structure):
+    _fields_ = [("init_gsize", C.c_int32), ("nt", C.c_int32), ("n_wsamples", C.c_int32), ("n_modes", C.c_int32),
+                ("interpolate_degree", C.c_int32), ("obstacle_mode", C.c_int32), ("dt", C.c_double),
+                ("dxy", C.c_double), ("A", C.c_double), ("A_sc", C.c_double), ("eps", C.c_double),
+                ("w_lo", C.c_double), ("w_hi", C.c_double), ("wx", C.c_double), ("obs_upper_row", C.c_double),
+                ("obs_left_col", C.c_double), ("obs_width", C.c_double), ("obs_speed_x", C.c_double),
+                ("obs_speed_y", C.c_double)]
+
+
+class EnvFields(C.Structure):
+    _fields_ = [(n, C.c_void_p) for n in ("u", "v", "ui", "vi", "yi", "phi", "phi_i", "phi_yi", "s", "mask")]
+
+
+class EnvStats(C.Structure):
+    _fields_ = [("seconds", C.c_double), ("fine_gsize", C.c_int32), ("transposed_vel", C.c_int32),
+                ("transposed_phi", C.c_int32), ("reserved", C.c_int32)]
+
+
 # every exported symbol of include/e2e_dp.h with its signature
 SIGNATURES = {
     "e2e_abi_version": (C.c_int, []),
@@ -153,6 +174,8 @@ SIGNATURES = {
                               C.POINTER(RolloutStats), C.c_void_p]),
     "e2e_build_solve": (C.c_int, [C.POINTER(Problem), C.POINTER(Fields), C.c_int, C.c_void_p, C.c_void_p,
                                   C.c_int, C.POINTER(FusedStats), C.c_void_p]),
+    "e2e_env_generate": (C.c_int, [C.POINTER(EnvParams), C.c_void_p, C.c_void_p, C.c_int, C.POINTER(EnvFields),
+                                   C.c_void_p, C.POINTER(EnvStats), C.c_void_p]),
     "e2e_server_create": (C.c_int, [C.POINTER(ServerOpts), C.POINTER(C.c_void_p)]),
     "e2e_server_add_field": (C.c_int, [C.c_void_p, C.POINTER(Problem), C.POINTER(Fields), C.c_int,
                                        C.POINTER(C.c_int32)]),

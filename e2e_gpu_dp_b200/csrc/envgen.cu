@@ -1,0 +1,542 @@
+// Environment generator on the GPU: double-gyre realisations -> per-time
+// rank reduction -> interpolation to the planning grid, plus the moving
+// scalar "cloud" field and the obstacle mask
+// (src/data_input/build_environment_DG_with_westward_clouds.py:106-590).
+//
+// Per time step t (one at a time, so memory is one step's matrices):
+//   k_env_realisations  vx, vy, phi of every (sample k, coarse cell) in double,
+//                       the reference's expressions in its evaluation order
+//                       without contraction (:130-147, 20-84 for the cloud)
+//   k_env_center        column means in sample order (np.mean over axis 1 is a
+//                       sequential sum for this layout) and the centred matrix
+//   SVD                 of the centred matrix by one-sided Jacobi (cuSOLVER
+//                       gesvdj, economy size): singular values to about
+//                       machine precision relative to the largest, like
+//                       np.linalg.svd's LAPACK (a Gram-matrix eigensolve would
+//                       lose (s_1/s_k)^2 of it, and s_4/s_1 ~ 1e-6 here); the
+//                       first n_modes give coefficients u_k s_k and modes v_k,
+//                       signs fixed so that each coefficient column's
+//                       largest-magnitude entry is positive (the reference's
+//                       np.linalg.svd leaves the sign to LAPACK)
+// then, for all steps, k_env_interpolate: the reference's griddata 'linear' on
+// the coarse cell centres, evaluated from a table of (triangle vertices,
+// barycentric weights) per fine point that the caller builds from the same
+// Delaunay triangulation (scipy's), summed in griddata's order in double
+// without contraction; points outside the hull read 0 (np.nan_to_num of the
+// fill value).
+#include <cuda_runtime.h>
+#include <cusolverDn.h>
+#include <math.h>
+
+#include <algorithm>
+#include <string>
+#include <vector>
+
+#include "e2e_dp.h"
+#include "internal.h"
+
+using namespace e2e;
+
+#define CK(call)                                        \
+  do {                                                  \
+    cudaError_t _e = (call);                            \
+    if (_e != cudaSuccess) return cuda_fail(_e, #call); \
+  } while (0)
+#define CKS(call)                                                                           \
+  do {                                                                                      \
+    cusolverStatus_t _s = (call);                                                           \
+    if (_s != CUSOLVER_STATUS_SUCCESS)                                                      \
+      return fail(E2E_ERR_CUDA, std::string(#call) + ": cuSOLVER status " + std::to_string((int)_s)); \
+  } while (0)
+
+namespace {
+
+constexpr double kPi = 3.141592653589793;  // math.pi
+
+__device__ __forceinline__ double mul(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ double add(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ double sub(double a, double b) { return __dsub_rn(a, b); }
+
+struct RealArgs {
+  int g, nws, t;
+  double tt;  // ts[t] = t * dt
+  double dxy, A, eps, wlo, whi, wx, wy;
+  double* Xv;  // nws x 2n: vx then vy
+  double* Xp;  // nws x n: phi
+};
+
+// DG_velocity_field.vx_vy / phi / sample_w / get_ij_from_xy (:130-166)
+__global__ void k_env_realisations(RealArgs a) {
+  const int n = a.g * a.g;
+  const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= (int64_t)a.nws * n) return;
+  const int k = (int)(idx / n), c = (int)(idx - (int64_t)k * n);
+  const int i = c / a.g, j = c - i * a.g;
+  // w = w_i + r (w_f - w_i), r = k / (n_wsamples - 1)
+  const double r = a.nws > 1 ? (double)k / (double)(a.nws - 1) : 0.0;
+  const double w = add(a.wlo, mul(r, sub(a.whi, a.wlo)));
+  const double x = mul(add(0.5, (double)j), a.dxy);
+  const double y = mul(add(0.5, (double)(a.g - 1 - i)), a.dxy);
+  const double swt = sin(mul(w, a.tt));
+  // f = eps sin(wt) x^2 + (1 - 2 eps sin(wt)) x;  fx = 2 eps sin(wt) (x - 1) + 1
+  const double term1 = mul(mul(a.eps, swt), mul(x, x));
+  const double e2s = mul(mul(2.0, a.eps), swt);
+  const double term2 = mul(sub(1.0, e2s), x);
+  const double f = add(term1, term2);
+  const double fx = add(mul(e2s, sub(x, 1.0)), 1.0);
+  const double swf = sin(mul(a.wx, f)), cwf = cos(mul(a.wx, f));
+  const double swy = sin(mul(a.wy, y)), cwy = cos(mul(a.wy, y));
+  const double vx = -mul(mul(mul(mul(0.5, a.A), kPi), swf), cwy);
+  const double vy = mul(mul(mul(mul(a.A, kPi), swy), fx), cwf);
+  const double ph = mul(mul(a.A, sin(mul(kPi, f))), swy);
+  a.Xv[(int64_t)k * 2 * n + c] = vx;
+  a.Xv[(int64_t)k * 2 * n + n + c] = vy;
+  a.Xp[(int64_t)k * n + c] = ph;
+}
+
+// column means (sequential sum over samples, then / n_wsamples) and centring
+__global__ void k_env_center(double* X, int nws, int ncols, double* mean) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= ncols) return;
+  double s = X[c];
+  for (int k = 1; k < nws; ++k) s = add(s, X[(int64_t)k * ncols + c]);
+  const double m = __ddiv_rn(s, (double)nws);
+  mean[c] = m;
+  for (int k = 0; k < nws; ++k) X[(int64_t)k * ncols + c] = sub(X[(int64_t)k * ncols + c], m);
+}
+
+// From the SVD of the centred matrix X (nws x ncols): coefficients C (nws x r)
+// and modes M (r x ncols), mode q = the q-th largest singular value:
+// C[k][q] = Us[k + q ldu] s_q (the left singular vectors scaled, rank_reduction's
+// u1 diag(s1)), M[q][c] = Vs[c + q ldv] (Vh's rows).  Signs: the
+// largest-magnitude coefficient of each mode is made positive.
+struct ModeArgs {
+  int nws, ncols, r;
+  const double* S;   // singular values, descending
+  const double* Us;  // left singular vectors (sample side), column q at Us + q * ldu
+  int ldu;
+  const double* Vs;  // right singular vectors (grid side), column q at Vs + q * ldv
+  int ldv;
+  double* C;         // nws x r
+  double* M;         // r x ncols
+  double* svals;     // r
+};
+
+__global__ void k_env_modes(ModeArgs a) {
+  const int q = blockIdx.x;  // one block per mode
+  const double s = a.S[q];
+  __shared__ double best_v[32];
+  __shared__ int best_k[32];
+  const double* u = a.Us + (int64_t)q * a.ldu;
+  double bv = -1.0;
+  int bk = 0x7fffffff;
+  for (int k = threadIdx.x; k < a.nws; k += blockDim.x) {
+    const double v = fabs(u[k] * s);
+    if (v > bv || (v == bv && k < bk)) {
+      bv = v;
+      bk = k;
+    }
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    const double ov = __shfl_xor_sync(0xffffffffu, bv, o);
+    const int ok = __shfl_xor_sync(0xffffffffu, bk, o);
+    if (ov > bv || (ov == bv && ok < bk)) {
+      bv = ov;
+      bk = ok;
+    }
+  }
+  if ((threadIdx.x & 31) == 0) {
+    best_v[threadIdx.x >> 5] = bv;
+    best_k[threadIdx.x >> 5] = bk;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int w = 1; w < (int)(blockDim.x >> 5); ++w)
+      if (best_v[w] > bv || (best_v[w] == bv && best_k[w] < bk)) {
+        bv = best_v[w];
+        bk = best_k[w];
+      }
+    best_k[0] = bk;
+  }
+  __syncthreads();
+  const double sgn = u[best_k[0]] < 0.0 ? -1.0 : 1.0;
+  if (threadIdx.x == 0) a.svals[q] = s;
+  for (int k = threadIdx.x; k < a.nws; k += blockDim.x) a.C[(int64_t)k * a.r + q] = sgn * (u[k] * s);
+  const double* v = a.Vs + (int64_t)q * a.ldv;
+  for (int c = threadIdx.x; c < a.ncols; c += blockDim.x) a.M[(int64_t)q * a.ncols + c] = sgn * v[c];
+}
+
+// row-major nws x ncols -> column-major (ld nws)
+__global__ void k_env_transpose(const double* X, int nws, int ncols, double* B) {
+  const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= (int64_t)nws * ncols) return;
+  const int k = (int)(idx / ncols), c = (int)(idx - (int64_t)k * ncols);
+  B[(int64_t)c * nws + k] = X[idx];
+}
+
+// coarse arrays of step t: [u, v, phi, ui_0.., vi_0.., phi_i_0..] (3 + 3r arrays
+// of n) and the coefficients of both rank reductions.  The reference holds the
+// coarse means and modes in float32 arrays except all_phi_mat, a float64 array
+// (:271), so every value but phi's mean is rounded to float before it is
+// interpolated.
+__global__ void k_env_store(int n, int nws, int r, const double* mv, const double* mp, const double* Mv,
+                            const double* Mp, const double* Cv, const double* Cp, double* coarse, float* yi,
+                            float* phi_yi) {
+  const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int64_t nb = (int64_t)(3 + 3 * r) * n;
+  if (idx < nb) {
+    const int b = (int)(idx / n), c = (int)(idx - (int64_t)b * n);
+    double v;
+    if (b == 0) v = mv[c];
+    else if (b == 1) v = mv[n + c];
+    else if (b == 2) v = mp[c];
+    else if (b < 3 + r) v = Mv[(int64_t)(b - 3) * 2 * n + c];
+    else if (b < 3 + 2 * r) v = Mv[(int64_t)(b - 3 - r) * 2 * n + n + c];
+    else v = Mp[(int64_t)(b - 3 - 2 * r) * n + c];
+    coarse[idx] = b == 2 ? v : (double)(float)v;
+  }
+  const int64_t nc = (int64_t)nws * r;
+  if (idx < nc) {
+    yi[idx] = (float)Cv[idx];
+    phi_yi[idx] = (float)Cp[idx];
+  }
+}
+
+struct InterpArgs {
+  int nt, r, n, G2;
+  const double* coarse;  // nt x (3 + 3r) x n
+  const int32_t* vert;   // G2 x 3 (vert[0] < 0: outside the hull)
+  const double* wgt;     // G2 x 3
+  float *u, *v, *phi, *ui, *vi, *phi_i;
+};
+
+// LinearNDInterpolator's evaluation (scipy/interpolate/_interpnd.pyx
+// _do_evaluate): out = 0; out += c_j * value[vertex_j] for j = 0..2 in double
+__global__ void k_env_interpolate(InterpArgs a) {
+  const int nb = 3 + 3 * a.r;
+  const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= (int64_t)a.nt * nb * a.G2) return;
+  const int p = (int)(idx % a.G2);
+  const int64_t tb = idx / a.G2;
+  const int b = (int)(tb % nb), t = (int)(tb / nb);
+  const double* src = a.coarse + ((int64_t)t * nb + b) * a.n;
+  float out = 0.f;  // np.nan_to_num of the fill value outside the hull
+  const int v0 = a.vert[3 * p];
+  if (v0 >= 0) {
+    double o = 0.0;
+    o = add(o, mul(a.wgt[3 * p + 0], src[v0]));
+    o = add(o, mul(a.wgt[3 * p + 1], src[a.vert[3 * p + 1]]));
+    o = add(o, mul(a.wgt[3 * p + 2], src[a.vert[3 * p + 2]]));
+    out = isnan(o) ? 0.f : (float)o;
+  }
+  float* dst;
+  if (b == 0) dst = a.u + (int64_t)t * a.G2;
+  else if (b == 1) dst = a.v + (int64_t)t * a.G2;
+  else if (b == 2) dst = a.phi + (int64_t)t * a.G2;
+  else if (b < 3 + a.r) dst = a.ui + ((int64_t)t * a.r + (b - 3)) * a.G2;
+  else if (b < 3 + 2 * a.r) dst = a.vi + ((int64_t)t * a.r + (b - 3 - a.r)) * a.G2;
+  else dst = a.phi_i + ((int64_t)t * a.r + (b - 3 - 2 * a.r)) * a.G2;
+  dst[p] = out;
+}
+
+// DG_scalar_field.generate_phi (:20-98) on the fine grid (its interpolate_degree
+// is the default 1, so T = t / 2), and fill_obstacles (:441-468)
+struct CloudArgs {
+  int nt, G;
+  double dxy;  // fine spacing
+  double A_sc;
+  int obst_mode;
+  double ou, ol, ow, osx, osy;
+  float* s;
+  int32_t* mask;
+};
+
+__global__ void k_env_cloud(CloudArgs a) {
+  const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int64_t G2 = (int64_t)a.G * a.G;
+  if (idx >= (int64_t)a.nt * G2) return;
+  const int t = (int)(idx / G2);
+  const int p = (int)(idx - (int64_t)t * G2);
+  const int i = p / a.G, j = p - i * a.G;
+  const double x = mul(add(0.5, (double)j), a.dxy);
+  const double xl = mul(add(0.5, (double)(a.G - 1)), a.dxy);  // xs[-1]
+  const double T = __ddiv_rn((double)t, 2.0);
+  const double l = __ddiv_rn(xl, 2.0);
+  const double dom = add(xl, a.dxy);
+  const double xt = add(x, mul(T, a.dxy));
+  double f;
+  if (xt <= l) {
+    f = 1.0;
+  } else if (l < xt && xt < add(l, mul(0.2, dom))) {
+    const double slope = __ddiv_rn(1.0, mul(-0.2, dom));
+    f = add(1.0, mul(slope, sub(x, sub(l, mul(T, a.dxy)))));
+  } else {
+    f = 0.0;
+  }
+  a.s[idx] = (float)mul(a.A_sc, f);
+  int m = 0;
+  if (a.obst_mode == E2E_OBST_STATIC) {
+    const int ru = (int)(0.4 * a.G), rd = (int)(0.5 * a.G), cl = (int)(0.5 * a.G), cr = (int)(0.6 * a.G);
+    m = (i >= ru && i < rd && j >= cl && j < cr) ? 1 : 0;
+  } else if (a.obst_mode == E2E_OBST_DYNAMIC) {
+    const double clf = floor(add(a.ol, mul((double)t, a.osx)));
+    const double ruf = floor(add(a.ou, mul((double)t, a.osy)));
+    const double crf = trunc(add(clf, a.ow)), rdf = trunc(add(ruf, a.ow));
+    const double hi = (double)(a.G - 1);
+    const bool inside = (0.0 < clf && clf < hi) && (0.0 < crf && crf < hi) && (0.0 < ruf && ruf < hi) &&
+                        (0.0 < rdf && rdf < hi);
+    m = (inside && i >= (int)ruf && i < (int)rdf && j >= (int)clf && j < (int)crf) ? 1 : 0;
+  }
+  a.mask[idx] = m;
+}
+
+// Truncated SVD of the centred nws x ncols matrix X (row-major, on the device;
+// destroyed) by one-sided Jacobi (cuSOLVER gesvdj, economy size, sorted): the
+// row-major buffer is the column-major ncols x nws matrix X^T, which gesvdj
+// takes directly when ncols >= nws (X^T = U S V^T: X's left vectors are V);
+// otherwise X is transposed into column-major nws x ncols first.
+struct SvdWork {
+  cusolverDnHandle_t sol = nullptr;
+  gesvdjInfo_t params = nullptr;
+  double* B = nullptr;  // transposed copy (nws > ncols)
+  double* U = nullptr;  // m x min(m, n)
+  double* V = nullptr;  // n x min(m, n)
+  double* S = nullptr;  // min(m, n)
+  double* work = nullptr;
+  int lwork = 0;
+  int* info = nullptr;
+};
+
+e2e_status svd_shape(int nws, int ncols, int* m, int* n) {
+  if (ncols >= nws) {
+    *m = ncols;
+    *n = nws;
+  } else {
+    *m = nws;
+    *n = ncols;
+  }
+  return E2E_OK;
+}
+
+e2e_status truncated_svd(SvdWork& w, double* X, int nws, int ncols, int r, double* C, double* M, double* svals,
+                         cudaStream_t st) {
+  int m, n;
+  svd_shape(nws, ncols, &m, &n);
+  double* A = X;
+  if (ncols < nws) {
+    const int64_t tot = (int64_t)nws * ncols;
+    k_env_transpose<<<(unsigned)((tot + 255) / 256), 256, 0, st>>>(X, nws, ncols, w.B);
+    CK(cudaGetLastError());
+    A = w.B;
+  }
+  CKS(cusolverDnDgesvdj(w.sol, CUSOLVER_EIG_MODE_VECTOR, 1, m, n, A, m, w.S, w.U, m, w.V, n, w.work, w.lwork, w.info,
+                        w.params));
+  int h_info = 0;
+  CK(cudaMemcpyAsync(&h_info, w.info, sizeof(int), cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  if (h_info != 0) return fail(E2E_ERR_DEVICE, "Jacobi SVD did not converge (info " + std::to_string(h_info) + ")");
+  ModeArgs a;
+  a.nws = nws;
+  a.ncols = ncols;
+  a.r = r;
+  a.S = w.S;
+  if (ncols >= nws) {  // X^T = U S V^T: sample side V (n = nws rows), grid side U (m = ncols rows)
+    a.Us = w.V;
+    a.ldu = n;
+    a.Vs = w.U;
+    a.ldv = m;
+  } else {             // X = U S V^T: sample side U (m = nws rows), grid side V (n = ncols rows)
+    a.Us = w.U;
+    a.ldu = m;
+    a.Vs = w.V;
+    a.ldv = n;
+  }
+  a.C = C;
+  a.M = M;
+  a.svals = svals;
+  k_env_modes<<<r, 256, 0, st>>>(a);
+  CK(cudaGetLastError());
+  return E2E_OK;
+}
+
+}  // namespace
+
+extern "C" e2e_status e2e_env_generate(const e2e_env_params* p, const int32_t* interp_vertices,
+                                       const double* interp_weights, int out_where, const e2e_env_fields* out,
+                                       double* svals_out, e2e_env_stats* stats, void* stream) {
+  if (!p || !out) return fail(E2E_ERR_INVALID, "null argument");
+  if (out_where != E2E_HOST && out_where != E2E_DEVICE) return fail(E2E_ERR_INVALID, "bad out_where");
+  const int g = p->init_gsize, nt = p->nt, nws = p->n_wsamples, r = p->n_modes, d = p->interpolate_degree;
+  if (g < 2 || nt < 1 || nws < 2 || r < 1 || d < 1)
+    return fail(E2E_ERR_INVALID, "init_gsize >= 2, nt >= 1, n_wsamples >= 2, n_modes >= 1, interpolate_degree >= 1");
+  const int n = g * g;
+  // the reference asserts n_modes <= min(nt, n_wsamples, 2 n) (:213); the scalar
+  // field's reduction needs n_modes <= min(n_wsamples, n) as well
+  if (r > nt || r > nws || r > n) return fail(E2E_ERR_INVALID, "n_modes above min(nt, n_wsamples, init_gsize^2)");
+  if (!interp_vertices || !interp_weights) return fail(E2E_ERR_INVALID, "null interpolation table");
+  if (p->obstacle_mode < E2E_OBST_NONE || p->obstacle_mode > E2E_OBST_DYNAMIC)
+    return fail(E2E_ERR_INVALID, "bad obstacle_mode");
+  if (!out->u || !out->v || !out->ui || !out->vi || !out->yi || !out->phi || !out->phi_i || !out->phi_yi ||
+      !out->s || !out->mask)
+    return fail(E2E_ERR_INVALID, "null output array");
+  const int64_t G = (int64_t)g * d, G2 = G * G;
+  if (G > 46340) return fail(E2E_ERR_UNSUPPORTED, "fine grid too large");
+  cudaStream_t st = (cudaStream_t)stream;
+  DeviceScratch scratch(st);
+
+  cudaEvent_t ev[2];
+  for (int k = 0; k < 2; ++k) CK(cudaEventCreate(&ev[k]));
+  struct EvFree {
+    cudaEvent_t* e;
+    ~EvFree() { for (int k = 0; k < 2; ++k) cudaEventDestroy(e[k]); }
+  } evfree{ev};
+  CK(cudaEventRecord(ev[0], st));
+
+  // the interpolation table on the device
+  int32_t* dvert = nullptr;
+  double* dwgt = nullptr;
+  CK(dalloc((void**)&dvert, sizeof(int32_t) * 3 * (size_t)G2, st));
+  scratch.add(dvert);
+  CK(dalloc((void**)&dwgt, sizeof(double) * 3 * (size_t)G2, st));
+  scratch.add(dwgt);
+  CK(cudaMemcpyAsync(dvert, interp_vertices, sizeof(int32_t) * 3 * (size_t)G2, cudaMemcpyDefault, st));
+  CK(cudaMemcpyAsync(dwgt, interp_weights, sizeof(double) * 3 * (size_t)G2, cudaMemcpyDefault, st));
+
+  // per-step matrices and the results of all steps
+  double *Xv, *Xp, *mv, *mp, *Cv, *Cp, *Mv, *Mp, *sv;
+  double* coarse;
+  float *yi, *phi_yi;
+  const int nb = 3 + 3 * r;
+  CK(dalloc((void**)&Xv, sizeof(double) * (size_t)nws * 2 * n, st));
+  scratch.add(Xv);
+  CK(dalloc((void**)&Xp, sizeof(double) * (size_t)nws * n, st));
+  scratch.add(Xp);
+  CK(dalloc((void**)&mv, sizeof(double) * 2 * (size_t)n, st));
+  scratch.add(mv);
+  CK(dalloc((void**)&mp, sizeof(double) * (size_t)n, st));
+  scratch.add(mp);
+  CK(dalloc((void**)&Cv, sizeof(double) * (size_t)nws * r, st));
+  scratch.add(Cv);
+  CK(dalloc((void**)&Cp, sizeof(double) * (size_t)nws * r, st));
+  scratch.add(Cp);
+  CK(dalloc((void**)&Mv, sizeof(double) * (size_t)r * 2 * n, st));
+  scratch.add(Mv);
+  CK(dalloc((void**)&Mp, sizeof(double) * (size_t)r * n, st));
+  scratch.add(Mp);
+  CK(dalloc((void**)&sv, sizeof(double) * 2 * (size_t)nt * r, st));
+  scratch.add(sv);
+  CK(dalloc((void**)&coarse, sizeof(double) * (size_t)nt * nb * n, st));
+  scratch.add(coarse);
+
+  // outputs (device: the caller's arrays; host: staged and copied at the end)
+  e2e_env_fields o = *out;
+  const size_t b2 = sizeof(float) * (size_t)nt * G2, bm = b2 * r, by = sizeof(float) * (size_t)nt * nws * r;
+  if (out_where == E2E_HOST) {
+    float** fp[9] = {&o.u, &o.v, &o.ui, &o.vi, &o.yi, &o.phi, &o.phi_i, &o.phi_yi, &o.s};
+    const size_t fb[9] = {b2, b2, bm, bm, by, b2, bm, by, b2};
+    for (int k = 0; k < 9; ++k) {
+      CK(dalloc((void**)fp[k], fb[k], st));
+      scratch.add(*fp[k]);
+    }
+    CK(dalloc((void**)&o.mask, sizeof(int32_t) * (size_t)nt * G2, st));
+    scratch.add(o.mask);
+  }
+  yi = o.yi;
+  phi_yi = o.phi_yi;
+
+  // Jacobi SVD work space (the larger of the two reductions)
+  SvdWork w;
+  struct SvdFree {
+    SvdWork* w;
+    ~SvdFree() {
+      if (w->params) cusolverDnDestroyGesvdjInfo(w->params);
+      if (w->sol) cusolverDnDestroy(w->sol);
+    }
+  } svdfree{&w};
+  if (cusolverDnCreate(&w.sol) != CUSOLVER_STATUS_SUCCESS) return fail(E2E_ERR_CUDA, "cusolverDnCreate");
+  CKS(cusolverDnSetStream(w.sol, st));
+  CKS(cusolverDnCreateGesvdjInfo(&w.params));
+  CKS(cusolverDnXgesvdjSetSortEig(w.params, 1));
+  {
+    size_t bu = 0, bv = 0, bs = 0, bb = 0;
+    for (int ncols : {2 * n, n}) {
+      int m, k;
+      svd_shape(nws, ncols, &m, &k);
+      bu = std::max(bu, (size_t)m * k);
+      bv = std::max(bv, (size_t)k * k);
+      bs = std::max(bs, (size_t)k);
+      if (ncols < nws) bb = std::max(bb, (size_t)nws * ncols);
+    }
+    CK(dalloc((void**)&w.U, sizeof(double) * bu, st));
+    scratch.add(w.U);
+    CK(dalloc((void**)&w.V, sizeof(double) * bv, st));
+    scratch.add(w.V);
+    CK(dalloc((void**)&w.S, sizeof(double) * bs, st));
+    scratch.add(w.S);
+    if (bb) {
+      CK(dalloc((void**)&w.B, sizeof(double) * bb, st));
+      scratch.add(w.B);
+    }
+    CK(dalloc((void**)&w.info, sizeof(int), st));
+    scratch.add(w.info);
+    for (int ncols : {2 * n, n}) {
+      int m, k, lw = 0;
+      svd_shape(nws, ncols, &m, &k);
+      CKS(cusolverDnDgesvdj_bufferSize(w.sol, CUSOLVER_EIG_MODE_VECTOR, 1, m, k, Xv, m, w.S, w.U, m, w.V, k, &lw,
+                                       w.params));
+      w.lwork = std::max(w.lwork, lw);
+    }
+    CK(dalloc((void**)&w.work, sizeof(double) * (size_t)std::max(w.lwork, 1), st));
+    scratch.add(w.work);
+  }
+
+  for (int t = 0; t < nt; ++t) {
+    RealArgs ra{g, nws, t, (double)t * p->dt, p->dxy, p->A, p->eps, p->w_lo, p->w_hi, p->wx, 0.5 * kPi, Xv, Xp};
+    const int64_t nr = (int64_t)nws * n;
+    k_env_realisations<<<(unsigned)((nr + 255) / 256), 256, 0, st>>>(ra);
+    CK(cudaGetLastError());
+    k_env_center<<<(2 * n + 127) / 128, 128, 0, st>>>(Xv, nws, 2 * n, mv);
+    k_env_center<<<(n + 127) / 128, 128, 0, st>>>(Xp, nws, n, mp);
+    CK(cudaGetLastError());
+    e2e_status s = truncated_svd(w, Xv, nws, 2 * n, r, Cv, Mv, sv + (int64_t)t * r, st);
+    if (s != E2E_OK) return s;
+    s = truncated_svd(w, Xp, nws, n, r, Cp, Mp, sv + (int64_t)(nt + t) * r, st);
+    if (s != E2E_OK) return s;
+    const int64_t ns = std::max<int64_t>((int64_t)nb * n, (int64_t)nws * r);
+    k_env_store<<<(unsigned)((ns + 255) / 256), 256, 0, st>>>(n, nws, r, mv, mp, Mv, Mp, Cv, Cp,
+                                                                coarse + (int64_t)t * nb * n,
+                                                                yi + (int64_t)t * nws * r,
+                                                                phi_yi + (int64_t)t * nws * r);
+    CK(cudaGetLastError());
+  }
+  InterpArgs ia{nt, r, n, (int)G2, coarse, dvert, dwgt, o.u, o.v, o.phi, o.ui, o.vi, o.phi_i};
+  const int64_t ni = (int64_t)nt * nb * G2;
+  k_env_interpolate<<<(unsigned)((ni + 255) / 256), 256, 0, st>>>(ia);
+  CK(cudaGetLastError());
+  CloudArgs ca{nt, (int)G, p->dxy / d, p->A_sc, p->obstacle_mode, p->obs_upper_row, p->obs_left_col,
+               p->obs_width, p->obs_speed_x, p->obs_speed_y, o.s, o.mask};
+  const int64_t nc = (int64_t)nt * G2;
+  k_env_cloud<<<(unsigned)((nc + 255) / 256), 256, 0, st>>>(ca);
+  CK(cudaGetLastError());
+  CK(cudaEventRecord(ev[1], st));
+
+  if (out_where == E2E_HOST) {
+    float* const* fp[9] = {&o.u, &o.v, &o.ui, &o.vi, &o.yi, &o.phi, &o.phi_i, &o.phi_yi, &o.s};
+    float* const hp[9] = {out->u, out->v, out->ui, out->vi, out->yi, out->phi, out->phi_i, out->phi_yi, out->s};
+    const size_t fb[9] = {b2, b2, bm, bm, by, b2, bm, by, b2};
+    for (int k = 0; k < 9; ++k) CK(cudaMemcpyAsync(hp[k], *fp[k], fb[k], cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(out->mask, o.mask, sizeof(int32_t) * (size_t)nt * G2, cudaMemcpyDeviceToHost, st));
+  }
+  if (svals_out) CK(cudaMemcpyAsync(svals_out, sv, sizeof(double) * 2 * (size_t)nt * r, cudaMemcpyDefault, st));
+  CK(cudaStreamSynchronize(st));
+  if (stats) {
+    float ms = 0.f;
+    CK(cudaEventElapsedTime(&ms, ev[0], ev[1]));
+    stats->seconds = ms * 1e-3;
+    stats->fine_gsize = (int32_t)G;
+    stats->transposed_vel = 2 * n < nws ? 1 : 0;
+    stats->transposed_phi = n < nws ? 1 : 0;
+    stats->reserved = 0;
+  }
+  return E2E_OK;
+}

@@ -368,6 +368,47 @@ e2e_status e2e_build_solve(const e2e_problem* p, const e2e_fields* fields, int f
                            int32_t* policy_out, float* value_out, int out_where,
                            e2e_fused_stats* stats /* may be NULL */, void* stream);
 
+/* ---- environment generator (replaces build_environment_DG_with_westward_clouds,
+ * src/data_input/build_environment_DG_with_westward_clouds.py:510-590) --------
+ * Double-gyre velocity realisations for n_wsamples frequencies w in w_range on
+ * an init_gsize grid, per time step a rank-n_modes reduction of the centred
+ * realisations (mean = all_u_mat/all_v_mat, modes = all_ui_mat/all_vi_mat,
+ * coefficients = all_Yi; the same for the scalar field phi), interpolation of
+ * means and modes to the init_gsize*interpolate_degree grid, the moving scalar
+ * cloud (all_s_mat) and the obstacle mask.  The reference's scipy griddata
+ * 'linear' is evaluated from a table the caller provides: per fine point
+ * (row-major over the fine grid, as griddata's (xgrid, ygrid) points) the three
+ * vertex indices of its Delaunay triangle over the coarse cell centres (-1: outside
+ * the hull, value 0) and their barycentric weights, as scipy computes them
+ * (e2e_gpu_dp_b200.envgen.interp_table builds it).  Modes are defined up to sign:
+ * each mode's largest-magnitude coefficient is made positive (products of modes
+ * and coefficients, which is all the builder reads, do not depend on it).
+ * Outputs: nt x G x G (u, v, phi, s, mask), nt x n_modes x G x G (ui, vi, phi_i),
+ * nt x n_wsamples x n_modes (yi, phi_yi); G = init_gsize * interpolate_degree. */
+enum { E2E_OBST_NONE = 0, E2E_OBST_STATIC = 1, E2E_OBST_DYNAMIC = 2 };
+typedef struct {
+  int32_t init_gsize, nt, n_wsamples, n_modes, interpolate_degree;
+  int32_t obstacle_mode;   /* E2E_OBST_*: fill_obstacles (:441-468) */
+  double dt, dxy, A, A_sc, eps, w_lo, w_hi, wx;
+  double obs_upper_row, obs_left_col, obs_width, obs_speed_x, obs_speed_y; /* dynamic obstacle */
+} e2e_env_params;
+typedef struct {
+  float *u, *v, *ui, *vi, *yi, *phi, *phi_i, *phi_yi, *s;
+  int32_t* mask;
+} e2e_env_fields;
+typedef struct {
+  double seconds;          /* device time (CUDA events) */
+  int32_t fine_gsize;
+  int32_t transposed_vel;  /* 1: more samples than columns, the matrix was transposed for the SVD */
+  int32_t transposed_phi;
+  int32_t reserved;
+} e2e_env_stats;
+/* interp_vertices / interp_weights: (G*G) x 3, host or device memory.
+ * svals_out (may be NULL): 2 x nt x n_modes singular values (velocity, then phi). */
+e2e_status e2e_env_generate(const e2e_env_params* p, const int32_t* interp_vertices,
+                            const double* interp_weights, int out_where, const e2e_env_fields* out,
+                            double* svals_out, e2e_env_stats* stats /* may be NULL */, void* stream);
+
 /* ---- solve without device allocation ----------------------------------------
  * No counterpart in the reference.  For callers that cannot allocate device
  * memory (a serving loop whose memory is fully reserved by its own pool, or code
