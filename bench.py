@@ -676,6 +676,43 @@ def run_served(rates=(50, 200, 500, 1000, 2000), seconds_per_rate=10.0, max_requ
     }
 
 
+def run_envgen() -> dict:
+    """The environment generator at the reference script's parameters (25 x 25
+    coarse grid interpolated 8x to 200 x 200, nt=10, 1000 realisations, 3
+    modes): GPU time of e2e_env_generate, and the CPU restatement of the
+    reference generator (pure-Python realisations, numpy SVD, scipy griddata)
+    timed on two of the ten time steps and scaled to ten."""
+    import torch
+
+    from e2e_gpu_dp_b200 import envgen
+    from oracle import envgen as OE
+
+    cfg = envgen.reference_defaults()
+    cfg["dyn_obstacle_data"] = ("None",)
+    envgen.build_environment_DG_with_westward_clouds(**cfg)  # warm-up (library, solver handles)
+    runs = []
+    for _ in range(3):
+        t0 = time.perf_counter()
+        out = envgen.build_environment_DG_with_westward_clouds(device=True, **cfg)
+        torch.cuda.synchronize()
+        runs.append((time.perf_counter() - t0, out["stats"]["seconds"]))
+    wall = statistics.median(r[0] for r in runs)
+    dev = statistics.median(r[1] for r in runs)
+    res = {"config": "init_gsize 25, interpolate_degree 8 (200x200), nt 10, n_wsamples 1000, n_modes 3",
+           "device_s": round(dev, 4), "wall_s": round(wall, 4),
+           "svals_vel_t1": [round(float(x), 6) for x in out["svals_vel"][1]]}
+    sample = dict(cfg)
+    sample.pop("op_nrzns")
+    sample["nt"] = 2
+    sample["n_modes"] = 2  # the reference asserts n_modes <= nt
+    t0 = time.perf_counter()
+    OE.generate(**sample)
+    cpu_s = (time.perf_counter() - t0) * cfg["nt"] / sample["nt"]
+    res.update({"cpu_restatement_s_extrapolated": round(cpu_s, 2), "cpu_sample": "2 of 10 time steps",
+                "speedup_vs_cpu": round(cpu_s / wall, 1)})
+    return res
+
+
 def run_precision() -> dict:
     """Precision form: 300x300 grid, nt=150 (13.5 M states), 16 headings,
     nrzns 2000, 8 modes; uint16 counts with int32 next states, FP32 values, the
@@ -839,6 +876,8 @@ def main():
     ap.add_argument("--precision-only", action="store_true", help="only the precision form (300x300x150)")
     ap.add_argument("--no-precision", action="store_true", help="skip the precision form")
     ap.add_argument("--no-served", action="store_true", help="skip the served form")
+    ap.add_argument("--envgen-only", action="store_true", help="only the environment generator")
+    ap.add_argument("--no-envgen", action="store_true", help="skip the environment generator")
     args = ap.parse_args()
     if args.profile_case:
         return profile_case()
@@ -852,6 +891,9 @@ def main():
         return 0
     if args.precision_only:
         print(json.dumps({"precision": run_precision()}), flush=True)
+        return 0
+    if args.envgen_only:
+        print(json.dumps({"envgen": run_envgen()}), flush=True)
         return 0
     ws, rank, local = _dist()
     if args.impl == "reference":
@@ -873,6 +915,8 @@ def main():
             line["served"] = run_served()
         if rank == 0 and ws == 1 and not args.no_precision:
             line["precision"] = run_precision()
+        if rank == 0 and ws == 1 and not args.no_envgen:
+            line["envgen"] = run_envgen()
         if rank == 0:
             print(json.dumps(line), flush=True)
     finally:
