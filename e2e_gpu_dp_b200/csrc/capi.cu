@@ -399,12 +399,12 @@ extern "C" e2e_status e2e_build_model(const e2e_problem* p, const e2e_fields* f,
 
   DeviceScratch scratch(st);
   FieldsOnDevice fd;
-  s = fields_to_device(p, f, where, st, &fd, &scratch);
+  s = fields_to_device(p, f, where, st, &fd, &scratch, /*defer=*/true);
   if (s != E2E_OK) return s;
 
   e2e_model* m = new (std::nothrow) e2e_model();
   if (!m) return fail(E2E_ERR_NOMEM, "host allocation");
-  s = run_build(p, fd.F, plan, st, &scratch, m);
+  s = run_build(p, fd, plan, st, &scratch, m);
   if (s != E2E_OK) {
     free_model_buffers(m);
     delete m;
@@ -445,7 +445,7 @@ e2e_status plan_build(const e2e_problem* p, int count_bits, int64_t stage_hint, 
 }
 
 e2e_status fields_to_device(const e2e_problem* p, const e2e_fields* f, int where,
-                            cudaStream_t st, FieldsOnDevice* fd, DeviceScratch* keep) {
+                            cudaStream_t st, FieldsOnDevice* fd, DeviceScratch* keep, bool defer) {
   const size_t nc = (size_t)p->gsize * p->gsize, nt = (size_t)p->nt, nm = (size_t)p->nmodes;
   const size_t b2 = sizeof(float) * nt * nc;
   const size_t bm = sizeof(float) * nt * nm * nc;
@@ -453,10 +453,22 @@ e2e_status fields_to_device(const e2e_problem* p, const e2e_fields* f, int where
   const void* src[7] = {f->u, f->v, f->ui, f->vi, f->yi, f->s, f->mask};
   const size_t bytes[7] = {b2, b2, bm, bm, by, b2, sizeof(int32_t) * nt * nc};
   void* dst[7];
+  const bool deferred = defer && where == E2E_HOST;
+  fd->nt = (int)nt;
   for (int k = 0; k < 7; ++k) {
     bool owned = false;
     if (!src[k]) {
       dst[k] = nullptr;
+      continue;
+    }
+    if (deferred) {  // allocate now, copy per range of time steps later
+      CK(dalloc(&dst[k], bytes[k] ? bytes[k] : 16, st));
+      keep->add(dst[k]);
+      fd->src[k] = src[k];
+      fd->dst[k] = dst[k];
+      fd->step_bytes[k] = bytes[k] / nt;
+      fd->n_deferred++;
+      fd->h2d_bytes += bytes[k];
       continue;
     }
     e2e_status s = upload(src[k], bytes[k], where, &dst[k], &owned, st);
@@ -474,8 +486,20 @@ e2e_status fields_to_device(const e2e_problem* p, const e2e_fields* f, int where
   return E2E_OK;
 }
 
-e2e_status run_build(const e2e_problem* p, const DevFields& F, const BuildPlan& pl,
+e2e_status copy_field_steps(const FieldsOnDevice& fd, int t0, int t1, cudaStream_t st) {
+  if (t1 <= t0) return E2E_OK;
+  for (int k = 0; k < 7; ++k) {
+    if (!fd.src[k]) continue;
+    const size_t off = fd.step_bytes[k] * (size_t)t0, n = fd.step_bytes[k] * (size_t)(t1 - t0);
+    CK(cudaMemcpyAsync(static_cast<char*>(fd.dst[k]) + off, static_cast<const char*>(fd.src[k]) + off, n,
+                       cudaMemcpyHostToDevice, st));
+  }
+  return E2E_OK;
+}
+
+e2e_status run_build(const e2e_problem* p, const FieldsOnDevice& fd, const BuildPlan& pl,
                      cudaStream_t st, DeviceScratch* scratch, e2e_model* m) {
+  const DevFields& F = fd.F;
   DevProblem D;
   e2e_status s = make_dev_problem(p, st, &D, scratch);
   if (s != E2E_OK) return s;
@@ -538,9 +562,45 @@ e2e_status run_build(const e2e_problem* p, const DevFields& F, const BuildPlan& 
     A.pool = pool;
     A.pool_units = pool_units;
     CK(cudaEventRecord(ev[0], st));
-    CK(launch_build_tiles(A, pl.count_bits, p->nt - 1, st));
+    if (attempt == 0 && fd.n_deferred) {
+      // host fields: copy the first layers' steps, build them while the rest
+      // is copied on a second stream, then build the remaining layers
+      const int la = std::max(1, std::min(p->nt - 1, (p->nt - 1) / 16));
+      e2e_status cs = copy_field_steps(fd, 0, la + 1, st);
+      if (cs != E2E_OK) return cs;
+      BuildArgs A0 = A;
+      CK(launch_build_tiles(A0, pl.count_bits, la, st));
+      m->build_launches++;
+      if (la < p->nt - 1) {
+        cudaStream_t cps = nullptr;
+        cudaEvent_t evs[2] = {nullptr, nullptr};
+        CK(cudaStreamCreateWithFlags(&cps, cudaStreamNonBlocking));
+        struct CopyFree {
+          cudaStream_t s;
+          cudaEvent_t* e;
+          ~CopyFree() {
+            for (int k = 0; k < 2; ++k)
+              if (e[k]) cudaEventDestroy(e[k]);
+            if (s) cudaStreamDestroy(s);
+          }
+        } cpfree{cps, evs};
+        for (int k = 0; k < 2; ++k) CK(cudaEventCreateWithFlags(&evs[k], cudaEventDisableTiming));
+        CK(cudaEventRecord(evs[0], st));  // the device buffers exist (stream-ordered allocations)
+        CK(cudaStreamWaitEvent(cps, evs[0], 0));
+        cs = copy_field_steps(fd, la + 1, p->nt, cps);
+        if (cs != E2E_OK) return cs;
+        CK(cudaEventRecord(evs[1], cps));
+        CK(cudaStreamWaitEvent(st, evs[1], 0));
+        BuildArgs A1 = A;
+        A1.t0 = la;
+        CK(launch_build_tiles(A1, pl.count_bits, p->nt - 1 - la, st));
+        m->build_launches++;
+      }
+    } else {
+      CK(launch_build_tiles(A, pl.count_bits, p->nt - 1, st));
+      m->build_launches++;
+    }
     CK(cudaEventRecord(ev[1], st));
-    m->build_launches++;
     CK(cudaMemcpyAsync(hc, ctr, sizeof(hc), cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
     bool again = false;

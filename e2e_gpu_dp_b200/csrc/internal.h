@@ -67,6 +67,13 @@ struct BuildPlan {
 struct FieldsOnDevice {
   DevFields F{};
   size_t h2d_bytes = 0;
+  // host fields uploaded later, a range of time steps at a time (fields_to_device
+  // with defer): per field the host source, its device buffer and the bytes of
+  // one time step (every field is time-major)
+  int n_deferred = 0, nt = 0;
+  const void* src[7] = {};
+  void* dst[7] = {};
+  size_t step_bytes[7] = {};
 };
 
 e2e_status validate_problem(const e2e_problem* p);
@@ -76,8 +83,12 @@ e2e_status make_dev_problem(const e2e_problem* p, cudaStream_t st, DevProblem* D
                             DeviceScratch* keep);
 e2e_status plan_build(const e2e_problem* p, int count_bits, int64_t stage_hint, BuildPlan* pl);
 e2e_status fields_to_device(const e2e_problem* p, const e2e_fields* f, int where, cudaStream_t st,
-                            FieldsOnDevice* fd, DeviceScratch* keep);
-e2e_status run_build(const e2e_problem* p, const DevFields& F, const BuildPlan& pl,
+                            FieldsOnDevice* fd, DeviceScratch* keep, bool defer = false);
+// copy time steps [t0, t1) of deferred host fields on stream st
+e2e_status copy_field_steps(const FieldsOnDevice& fd, int t0, int t1, cudaStream_t st);
+// the build; with deferred host fields the first layers' fields are copied
+// first and the rest overlaps the builder's first launch
+e2e_status run_build(const e2e_problem* p, const FieldsOnDevice& fd, const BuildPlan& pl,
                      cudaStream_t st, DeviceScratch* scratch, e2e_model* m);
 ViModel vi_model(const e2e_model* m);
 void free_model_buffers(e2e_model* m);
