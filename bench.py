@@ -18,6 +18,7 @@ Multi-GPU: independent replicas, one per rank (the workload does not shard).
 from __future__ import annotations
 
 import argparse
+import gc
 import json
 import os
 import statistics
@@ -277,12 +278,18 @@ def run_ours(args, ws, rank, local):
     recs = []
     starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
     ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    # the Python collector's pauses are host noise between launches: collect and
+    # freeze the objects made so far, and keep it off while steps are timed
+    gc.collect()
+    gc.freeze()
     with Clocks(local) as clk:
         for _ in range(args.warmup):
             step()
         torch.cuda.synchronize()
         _barrier(ws)
         clk.begin()
+        gc.collect()
+        gc.disable()
         torch.cuda.synchronize()
         # each step between its own events: the clock sample taken between two
         # steps (host only, GPU idle) is not part of either
@@ -293,6 +300,7 @@ def run_ours(args, ws, rank, local):
             torch.cuda.synchronize()
             clk.tick()
         torch.cuda.synchronize()
+        gc.enable()
     _barrier(ws)
     step_ms = [round(starts[k].elapsed_time(ends[k]), 2) for k in range(args.steps)]
     ms = _max_over_ranks(sum(starts[k].elapsed_time(ends[k]) for k in range(args.steps)) / args.steps, ws)
@@ -325,6 +333,8 @@ def run_ours(args, ws, rank, local):
         e2e_step()
     torch.cuda.synchronize()
     _barrier(ws)
+    gc.collect()
+    gc.disable()
     t0 = time.perf_counter()
     f0 = torch.cuda.Event(enable_timing=True)
     f1 = torch.cuda.Event(enable_timing=True)
@@ -336,6 +346,7 @@ def run_ours(args, ws, rank, local):
         e2e_steps.append(round((time.perf_counter() - te) * 1e3, 1))
     f1.record(stream)
     torch.cuda.synchronize()
+    gc.enable()
     e2e_ms = max(f0.elapsed_time(f1), (time.perf_counter() - t0) * 1e3) / args.steps
     e2e_ms = _max_over_ranks(e2e_ms, ws)
 

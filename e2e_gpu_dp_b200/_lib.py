@@ -140,7 +140,7 @@ class EnvFields(C.Structure):
 
 class EnvStats(C.Structure):
     _fields_ = [("seconds", C.c_double), ("fine_gsize", C.c_int32), ("transposed_vel", C.c_int32),
-                ("transposed_phi", C.c_int32), ("reserved", C.c_int32)]
+                ("transposed_phi", C.c_int32), ("full_svds", C.c_int32)]
 
 
 # every exported symbol of include/e2e_dp.h with its signature

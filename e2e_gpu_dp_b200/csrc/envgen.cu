@@ -9,8 +9,15 @@
 //                       without contraction (:130-147, 20-84 for the cloud)
 //   k_env_center        column means in sample order (np.mean over axis 1 is a
 //                       sequential sum for this layout) and the centred matrix
-//   SVD                 of the centred matrix by one-sided Jacobi (cuSOLVER
-//                       gesvdj, economy size): singular values to about
+//   SVD                 of the centred matrix, the leading n_modes triplets:
+//                       a randomized range finder (n_modes + 10 columns, two
+//                       power iterations, QR by cuSOLVER, products by cuBLAS)
+//                       and a one-sided Jacobi SVD (cuSOLVER gesvdj) of the
+//                       projected matrix, accepted when the explicit residual
+//                       |X - Q Q^T X|_F is below 1e-10 s_1 (then every kept
+//                       singular value is exact to ~|R|^2/s_k); otherwise, as
+//                       at t = 0 where X is rounding noise, gesvdj of the whole
+//                       matrix.  Either way singular values come to about
 //                       machine precision relative to the largest, like
 //                       np.linalg.svd's LAPACK (a Gram-matrix eigensolve would
 //                       lose (s_1/s_k)^2 of it, and s_4/s_1 ~ 1e-6 here); the
@@ -24,6 +31,7 @@
 // Delaunay triangulation (scipy's), summed in griddata's order in double
 // without contraction; points outside the hull read 0 (np.nan_to_num of the
 // fill value).
+#include <cublas_v2.h>
 #include <cuda_runtime.h>
 #include <cusolverDn.h>
 #include <math.h>
@@ -41,6 +49,12 @@ using namespace e2e;
   do {                                                  \
     cudaError_t _e = (call);                            \
     if (_e != cudaSuccess) return cuda_fail(_e, #call); \
+  } while (0)
+#define CKB(call)                                                                               \
+  do {                                                                                          \
+    cublasStatus_t _s = (call);                                                                 \
+    if (_s != CUBLAS_STATUS_SUCCESS)                                                            \
+      return fail(E2E_ERR_CUDA, std::string(#call) + ": cuBLAS status " + std::to_string((int)_s)); \
   } while (0)
 #define CKS(call)                                                                           \
   do {                                                                                      \
@@ -164,6 +178,18 @@ __global__ void k_env_modes(ModeArgs a) {
   for (int k = threadIdx.x; k < a.nws; k += blockDim.x) a.C[(int64_t)k * a.r + q] = sgn * (u[k] * s);
   const double* v = a.Vs + (int64_t)q * a.ldv;
   for (int c = threadIdx.x; c < a.ncols; c += blockDim.x) a.M[(int64_t)q * a.ncols + c] = sgn * v[c];
+}
+
+// test matrix of the range finder: deterministic values in [-1, 1) from a
+// 64-bit mix of the index (any matrix of full rank with the range works)
+__global__ void k_env_test_matrix(double* O, int64_t n) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  uint64_t z = (uint64_t)i * 0x9E3779B97F4A7C15ull + 0x632BE59BD9B4E019ull;
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+  z ^= z >> 31;
+  O[i] = (double)(z >> 11) * (2.0 / 9007199254740992.0) - 1.0;
 }
 
 // row-major nws x ncols -> column-major (ld nws)
@@ -297,7 +323,14 @@ __global__ void k_env_cloud(CloudArgs a) {
 // otherwise X is transposed into column-major nws x ncols first.
 struct SvdWork {
   cusolverDnHandle_t sol = nullptr;
+  cublasHandle_t blas = nullptr;
   gesvdjInfo_t params = nullptr;
+  // randomized range finder: k = r + oversampling columns
+  int k = 0;
+  double *Om = nullptr, *Q = nullptr, *Z = nullptr, *Bt = nullptr, *L = nullptr, *R = nullptr;
+  double *Ub = nullptr, *Vb = nullptr, *Sb = nullptr, *tau = nullptr;
+  double* qwork = nullptr;
+  int lqwork = 0;
   double* B = nullptr;  // transposed copy (nws > ncols)
   double* U = nullptr;  // m x min(m, n)
   double* V = nullptr;  // n x min(m, n)
@@ -318,8 +351,79 @@ e2e_status svd_shape(int nws, int ncols, int* m, int* n) {
   return E2E_OK;
 }
 
+// orthonormal basis of the column range of A (rows x k, column-major, ld rows), in place
+e2e_status orthonormalize(SvdWork& w, double* A, int rows, int k) {
+  CKS(cusolverDnDgeqrf(w.sol, rows, k, A, rows, w.tau, w.qwork, w.lqwork, w.info));
+  CKS(cusolverDnDorgqr(w.sol, rows, k, k, A, rows, w.tau, w.qwork, w.lqwork, w.info));
+  return E2E_OK;
+}
+
+// Randomized SVD of X (row-major nws x ncols, read only).  Returns false in
+// *ok when the residual check fails (the caller then runs gesvdj).
+e2e_status randomized_svd(SvdWork& w, const double* X, int nws, int ncols, int r, double* C, double* M,
+                          double* svals, bool* ok, cudaStream_t st) {
+  *ok = false;
+  const int k = std::min(w.k, std::min(nws, ncols));
+  if (k <= r || (int64_t)nws * ncols > (int64_t)0x7fffffff) return E2E_OK;
+  const double one = 1.0, zero = 0.0, mone = -1.0;
+  // X as the column-major ncols x nws matrix Xc (= X^T), ld ncols
+  const int64_t no = (int64_t)ncols * k;
+  k_env_test_matrix<<<(unsigned)((no + 255) / 256), 256, 0, st>>>(w.Om, no);
+  CK(cudaGetLastError());
+  // Q = X Om (nws x k)
+  CKB(cublasDgemm(w.blas, CUBLAS_OP_T, CUBLAS_OP_N, nws, k, ncols, &one, X, ncols, w.Om, ncols, &zero, w.Q, nws));
+  e2e_status s = orthonormalize(w, w.Q, nws, k);
+  if (s != E2E_OK) return s;
+  for (int it = 0; it < 2; ++it) {  // power iterations: Q <- orth(X orth(X^T Q))
+    CKB(cublasDgemm(w.blas, CUBLAS_OP_N, CUBLAS_OP_N, ncols, k, nws, &one, X, ncols, w.Q, nws, &zero, w.Z, ncols));
+    s = orthonormalize(w, w.Z, ncols, k);
+    if (s != E2E_OK) return s;
+    CKB(cublasDgemm(w.blas, CUBLAS_OP_T, CUBLAS_OP_N, nws, k, ncols, &one, X, ncols, w.Z, ncols, &zero, w.Q, nws));
+    s = orthonormalize(w, w.Q, nws, k);
+    if (s != E2E_OK) return s;
+  }
+  // Bt = X^T Q (ncols x k) = (Q^T X)^T
+  CKB(cublasDgemm(w.blas, CUBLAS_OP_N, CUBLAS_OP_N, ncols, k, nws, &one, X, ncols, w.Q, nws, &zero, w.Bt, ncols));
+  // residual X - Q Q^T X, as Xc - Bt Q^T, and its Frobenius norm
+  CK(cudaMemcpyAsync(w.R, X, sizeof(double) * (size_t)nws * ncols, cudaMemcpyDeviceToDevice, st));
+  CKB(cublasDgemm(w.blas, CUBLAS_OP_N, CUBLAS_OP_T, ncols, nws, k, &mone, w.Bt, ncols, w.Q, nws, &one, w.R, ncols));
+  double rnorm = 0.0;
+  CKB(cublasDnrm2(w.blas, nws * ncols, w.R, 1, &rnorm));  // host result: synchronises
+  // SVD of the tall Bt = Ub S Vb^T: X ~ Q B = (Q Vb) S Ub^T
+  CKS(cusolverDnDgesvdj(w.sol, CUSOLVER_EIG_MODE_VECTOR, 1, ncols, k, w.Bt, ncols, w.Sb, w.Ub, ncols, w.Vb, k,
+                        w.work, w.lwork, w.info, w.params));
+  int h_info = 0;
+  CK(cudaMemcpyAsync(&h_info, w.info, sizeof(int), cudaMemcpyDeviceToHost, st));
+  double s1 = 0.0;
+  CK(cudaMemcpyAsync(&s1, w.Sb, sizeof(double), cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  if (h_info != 0 || !(rnorm <= 1e-10 * s1) || !(s1 > 0.0)) return E2E_OK;
+  CKB(cublasDgemm(w.blas, CUBLAS_OP_N, CUBLAS_OP_N, nws, k, k, &one, w.Q, nws, w.Vb, k, &zero, w.L, nws));
+  ModeArgs a;
+  a.nws = nws;
+  a.ncols = ncols;
+  a.r = r;
+  a.S = w.Sb;
+  a.Us = w.L;
+  a.ldu = nws;
+  a.Vs = w.Ub;
+  a.ldv = ncols;
+  a.C = C;
+  a.M = M;
+  a.svals = svals;
+  k_env_modes<<<r, 256, 0, st>>>(a);
+  CK(cudaGetLastError());
+  *ok = true;
+  return E2E_OK;
+}
+
 e2e_status truncated_svd(SvdWork& w, double* X, int nws, int ncols, int r, double* C, double* M, double* svals,
-                         cudaStream_t st) {
+                         cudaStream_t st, int* full_svds) {
+  bool ok = false;
+  e2e_status rs = randomized_svd(w, X, nws, ncols, r, C, M, svals, &ok, st);
+  if (rs != E2E_OK) return rs;
+  if (ok) return E2E_OK;
+  ++*full_svds;
   int m, n;
   svd_shape(nws, ncols, &m, &n);
   double* A = X;
@@ -451,10 +555,14 @@ extern "C" e2e_status e2e_env_generate(const e2e_env_params* p, const int32_t* i
     ~SvdFree() {
       if (w->params) cusolverDnDestroyGesvdjInfo(w->params);
       if (w->sol) cusolverDnDestroy(w->sol);
+      if (w->blas) cublasDestroy(w->blas);
     }
   } svdfree{&w};
   if (cusolverDnCreate(&w.sol) != CUSOLVER_STATUS_SUCCESS) return fail(E2E_ERR_CUDA, "cusolverDnCreate");
   CKS(cusolverDnSetStream(w.sol, st));
+  if (cublasCreate(&w.blas) != CUBLAS_STATUS_SUCCESS) return fail(E2E_ERR_CUDA, "cublasCreate");
+  CKB(cublasSetStream(w.blas, st));
+  CKB(cublasSetPointerMode(w.blas, CUBLAS_POINTER_MODE_HOST));
   CKS(cusolverDnCreateGesvdjInfo(&w.params));
   CKS(cusolverDnXgesvdjSetSortEig(w.params, 1));
   {
@@ -486,9 +594,41 @@ extern "C" e2e_status e2e_env_generate(const e2e_env_params* p, const int32_t* i
                                        w.params));
       w.lwork = std::max(w.lwork, lw);
     }
+    // randomized range finder: k = n_modes + 10 columns
+    w.k = std::min(r + 10, std::min(nws, n));
+    const int kk = w.k, cmax = std::max(2 * n, nws);
+    double** rb[] = {&w.Om, &w.Z, &w.Bt, &w.Ub, &w.Q, &w.L};
+    for (double** b : rb) {
+      CK(dalloc((void**)b, sizeof(double) * (size_t)cmax * kk, st));
+      scratch.add(*b);
+    }
+    CK(dalloc((void**)&w.R, sizeof(double) * (size_t)nws * 2 * n, st));
+    scratch.add(w.R);
+    CK(dalloc((void**)&w.Vb, sizeof(double) * (size_t)kk * kk, st));
+    scratch.add(w.Vb);
+    CK(dalloc((void**)&w.Sb, sizeof(double) * (size_t)kk, st));
+    scratch.add(w.Sb);
+    CK(dalloc((void**)&w.tau, sizeof(double) * (size_t)kk, st));
+    scratch.add(w.tau);
+    for (int rows : {nws, 2 * n, n}) {
+      int lw = 0;
+      CKS(cusolverDnDgeqrf_bufferSize(w.sol, rows, kk, w.Q, rows, &lw));
+      w.lqwork = std::max(w.lqwork, lw);
+      CKS(cusolverDnDorgqr_bufferSize(w.sol, rows, kk, kk, w.Q, rows, w.tau, &lw));
+      w.lqwork = std::max(w.lqwork, lw);
+    }
+    for (int ncols : {2 * n, n}) {
+      int lw = 0;
+      CKS(cusolverDnDgesvdj_bufferSize(w.sol, CUSOLVER_EIG_MODE_VECTOR, 1, ncols, kk, w.Bt, ncols, w.Sb, w.Ub,
+                                       ncols, w.Vb, kk, &lw, w.params));
+      w.lwork = std::max(w.lwork, lw);
+    }
+    CK(dalloc((void**)&w.qwork, sizeof(double) * (size_t)std::max(w.lqwork, 1), st));
+    scratch.add(w.qwork);
     CK(dalloc((void**)&w.work, sizeof(double) * (size_t)std::max(w.lwork, 1), st));
     scratch.add(w.work);
   }
+  int full_svds = 0;
 
   for (int t = 0; t < nt; ++t) {
     RealArgs ra{g, nws, t, (double)t * p->dt, p->dxy, p->A, p->eps, p->w_lo, p->w_hi, p->wx, 0.5 * kPi, Xv, Xp};
@@ -498,9 +638,9 @@ extern "C" e2e_status e2e_env_generate(const e2e_env_params* p, const int32_t* i
     k_env_center<<<(2 * n + 127) / 128, 128, 0, st>>>(Xv, nws, 2 * n, mv);
     k_env_center<<<(n + 127) / 128, 128, 0, st>>>(Xp, nws, n, mp);
     CK(cudaGetLastError());
-    e2e_status s = truncated_svd(w, Xv, nws, 2 * n, r, Cv, Mv, sv + (int64_t)t * r, st);
+    e2e_status s = truncated_svd(w, Xv, nws, 2 * n, r, Cv, Mv, sv + (int64_t)t * r, st, &full_svds);
     if (s != E2E_OK) return s;
-    s = truncated_svd(w, Xp, nws, n, r, Cp, Mp, sv + (int64_t)(nt + t) * r, st);
+    s = truncated_svd(w, Xp, nws, n, r, Cp, Mp, sv + (int64_t)(nt + t) * r, st, &full_svds);
     if (s != E2E_OK) return s;
     const int64_t ns = std::max<int64_t>((int64_t)nb * n, (int64_t)nws * r);
     k_env_store<<<(unsigned)((ns + 255) / 256), 256, 0, st>>>(n, nws, r, mv, mp, Mv, Mp, Cv, Cp,
@@ -536,7 +676,7 @@ extern "C" e2e_status e2e_env_generate(const e2e_env_params* p, const int32_t* i
     stats->fine_gsize = (int32_t)G;
     stats->transposed_vel = 2 * n < nws ? 1 : 0;
     stats->transposed_phi = n < nws ? 1 : 0;
-    stats->reserved = 0;
+    stats->full_svds = full_svds;
   }
   return E2E_OK;
 }

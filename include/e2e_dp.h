@@ -401,7 +401,7 @@ typedef struct {
   int32_t fine_gsize;
   int32_t transposed_vel;  /* 1: more samples than columns, the matrix was transposed for the SVD */
   int32_t transposed_phi;
-  int32_t reserved;
+  int32_t full_svds;       /* reductions that fell back from the randomized SVD to the full Jacobi SVD */
 } e2e_env_stats;
 /* interp_vertices / interp_weights: (G*G) x 3, host or device memory.
  * svals_out (may be NULL): 2 x nt x n_modes singular values (velocity, then phi). */
