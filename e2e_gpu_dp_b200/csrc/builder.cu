@@ -44,6 +44,13 @@ enum : int { MASK_OVR = 0, MASK_INWIN = 1, MASK_EDGE = 2, MASK_TERM = 3, MASK_SL
 
 __device__ __forceinline__ bool bit64(uint64_t m, int b) { return (m >> b) & 1ull; }
 
+// bits lo..hi of a w-bit row (w <= 8), clipped to 0..w-1
+__device__ __forceinline__ uint32_t bit_range(int lo, int hi, int w) {
+  lo = max(lo, 0);
+  hi = min(hi, w - 1);
+  return lo > hi ? 0u : (((2u << hi) - 1u) & ~((1u << lo) - 1u));
+}
+
 static constexpr int kRcw = 64;                 // realisations per warp-private velocity chunk
 static constexpr int kVelStride = kRcw + 1;     // padded: the cells of a warp hit distinct banks
 static constexpr uint32_t kOvrFlag = 0x8000u;   // counter bit 15: bin is obstacle-overridden
@@ -219,15 +226,39 @@ __global__ void __launch_bounds__(1024) k_build_tiles(BuildArgs A) {
   }
   __syncthreads();
   // ---- obstacle override of S1 -> S2 for S2 within 6 cells of S1, per cell
-  // (goes_through_obstacle, src/build_model.cu:444-477), shared by the actions
-  for (int idx = tid; idx < 32 * kNbBits; idx += nthr) {
-    const int c = idx / kNbBits, b = idx - c * kNbBits;
-    const int64_t cc = c0 + c;
-    if (cc >= nc) continue;
-    const int ci1 = (int)(cc / g), cj1 = (int)(cc - (int64_t)ci1 * g);
-    const int i2 = ci1 + b / kNbSide - kNb, j2 = cj1 + b % kNbSide - kNb;
-    if (i2 < 0 || i2 >= g || j2 < 0 || j2 >= g) continue;
-    if (through_obstacle(P, A.F.mask, T, ci1, cj1, i2, j2)) atomicOr(&obsmap[c][b >> 5], 1u << (b & 31));
+  // (goes_through_obstacle, src/build_model.cu:444-477), shared by the actions.
+  // goes_through_obstacle(S1, S2) is the OR, over the obstacle cells o != S1
+  // (mask 1 at T or T+1) of the bounding box of S1 and S2, of within_band(o,
+  // S1, S2).  The loop runs the other way round: each obstacle cell o within 6
+  // cells of S1 tests every S2 whose box with S1 contains it (rows beyond o
+  // from S1, or all rows when o is on S1's row; the same for columns), so no
+  // box is scanned once per S2; the tests and the bits are the same.
+  {
+    const int32_t* mT = A.F.mask + (int64_t)T * nc;
+    for (int idx = tid; idx < 32 * kNbBits; idx += nthr) {
+      const int c = idx / kNbBits, ob = idx - c * kNbBits;
+      const int64_t cc = c0 + c;
+      if (cc >= nc) continue;
+      const int da = ob / kNbSide - kNb, db = ob % kNbSide - kNb;
+      if (da == 0 && db == 0) continue;
+      const int ci1 = (int)(cc / g), cj1 = (int)(cc - (int64_t)ci1 * g);
+      const int oi = ci1 + da, oj = cj1 + db;
+      if (oi < 0 || oi >= g || oj < 0 || oj >= g) continue;
+      const int64_t sp = (int64_t)oj + (int64_t)g * oi;
+      if (!(__ldg(mT + sp) == 1 || __ldg(mT + nc + sp) == 1)) continue;
+      const int dilo = da > 0 ? da : -kNb, dihi = da < 0 ? da : kNb;
+      const int djlo = db > 0 ? db : -kNb, djhi = db < 0 ? db : kNb;
+      for (int di = dilo; di <= dihi; ++di) {
+        const int i2 = ci1 + di;
+        if (i2 < 0 || i2 >= g) continue;
+        for (int dj = djlo; dj <= djhi; ++dj) {
+          const int j2 = cj1 + dj;
+          if (j2 < 0 || j2 >= g) continue;
+          const int tb = (di + kNb) * kNbSide + (dj + kNb);
+          if (within_band(P, oi, oj, ci1, cj1, i2, j2)) atomicOr(&obsmap[c][tb >> 5], 1u << (tb & 31));
+        }
+      }
+    }
   }
 
   // ---- per-row set-up -------------------------------------------------------
@@ -268,29 +299,50 @@ __global__ void __launch_bounds__(1024) k_build_tiles(BuildArgs A) {
     wj0 = min(max(cj - (kWin / 2 - 1), j1 - P.del), j1 + P.del - W + 1);
     wi0 = min(max(wi0, 0), g - W);
     wj0 = min(max(wj0, 0), g - W);
+    // Per window row, the bins (bit lj) in the m x m neighbourhood, on the grid
+    // edge, in the terminal subgrid, and obstacle-overridden; the columns of a
+    // row are contiguous bits of the obstacle bitmap when the row lies within 6
+    // cells of S1, otherwise each bin is tested as before.
+    const uint32_t colmask = (1u << W) - 1u;
+    const int dj0 = wj0 - j1;
+    const uint32_t cols_inw = bit_range(j1 - P.del - wj0, j1 + P.del - wj0, W);
+    const uint32_t cols_term = bit_range(P.jt - wj0, P.jt + P.tsg - 1 - wj0, W);
+    const uint32_t cols_edge = bit_range(-wj0, -wj0, W) | bit_range(g - 1 - wj0, g - 1 - wj0, W);
+    const bool bitmap_cols = dj0 >= -kNb && dj0 + W - 1 <= kNb;
+    uint64_t bins = 0;
     for (int li = 0; li < W; ++li) {
-      for (int lj = 0; lj < W; ++lj) {
-        const int i2 = wi0 + li, j2 = wj0 + lj;
-        const int b = li * kWin + lj;
-        const int di = i2 - i1, dj = j2 - j1;
-        const bool inw = di >= -P.del && di <= P.del && dj >= -P.del && dj <= P.del;
-        bool o;
-        if (di >= -kNb && di <= kNb && dj >= -kNb && dj <= kNb) {
-          const int nb = (di + kNb) * kNbSide + (dj + kNb);
-          o = (obsmap[cl][nb >> 5] >> (nb & 31)) & 1u;
-        } else {
-          o = through_obstacle(P, A.F.mask, T, i1, j1, i2, j2);
+      const int i2 = wi0 + li, di = i2 - i1;
+      const uint32_t r_inw = (di >= -P.del && di <= P.del) ? cols_inw : 0u;
+      const uint32_t r_edge = (i2 == 0 || i2 == g - 1) ? colmask : cols_edge;
+      const uint32_t r_term = (i2 >= P.it && i2 < P.it + P.tsg) ? cols_term : 0u;
+      uint32_t r_ovr = 0;
+      if (di >= -kNb && di <= kNb && bitmap_cols) {
+        const int q0 = (di + kNb) * kNbSide + (dj0 + kNb);
+        const int w0 = q0 >> 5;
+        const uint32_t lo = obsmap[cl][w0], hi = w0 + 1 < kNbWords ? obsmap[cl][w0 + 1] : 0u;
+        r_ovr = __funnelshift_r(lo, hi, q0 & 31) & colmask;
+      } else {
+        for (int lj = 0; lj < W; ++lj) {
+          const int j2 = wj0 + lj, dj = j2 - j1;
+          bool o;
+          if (di >= -kNb && di <= kNb && dj >= -kNb && dj <= kNb) {
+            const int nb = (di + kNb) * kNbSide + (dj + kNb);
+            o = (obsmap[cl][nb >> 5] >> (nb & 31)) & 1u;
+          } else {
+            o = through_obstacle(P, A.F.mask, T, i1, j1, i2, j2);
+          }
+          r_ovr |= (uint32_t)o << lj;
         }
-        if (inw) inwin |= 1ull << b;
-        if (o) {
-          ovr |= 1ull << b;
-          wcol[b << log2S] = (uint16_t)kOvrFlag;
-        }
-        if (i2 == 0 || i2 == g - 1 || j2 == 0 || j2 == g - 1) edge |= 1ull << b;
-        if (is_terminal(P, i2, j2)) term |= 1ull << b;
-        if (!inw || rad) slow |= 1ull << b;
       }
+      const int sh = li * kWin;
+      bins |= (uint64_t)colmask << sh;
+      inwin |= (uint64_t)r_inw << sh;
+      edge |= (uint64_t)r_edge << sh;
+      term |= (uint64_t)r_term << sh;
+      ovr |= (uint64_t)r_ovr << sh;
     }
+    slow = rad ? bins : (bins & ~inwin);
+    for (uint64_t mo = ovr; mo; mo &= mo - 1) wcol[(__ffsll((long long)mo) - 1) << log2S] = (uint16_t)kOvrFlag;
   }
   masks[MASK_OVR * nthr + tid] = ovr;
   masks[MASK_INWIN * nthr + tid] = inwin;
