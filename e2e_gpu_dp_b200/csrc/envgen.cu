@@ -233,6 +233,7 @@ struct InterpArgs {
   const double* coarse;  // nt x (3 + 3r) x n
   const int32_t* vert;   // G2 x 3 (vert[0] < 0: outside the hull)
   const double* wgt;     // G2 x 3
+  unsigned int* err;     // set when a vertex index is outside the coarse grid
   float *u, *v, *phi, *ui, *vi, *phi_i;
 };
 
@@ -247,13 +248,17 @@ __global__ void k_env_interpolate(InterpArgs a) {
   const int b = (int)(tb % nb), t = (int)(tb / nb);
   const double* src = a.coarse + ((int64_t)t * nb + b) * a.n;
   float out = 0.f;  // np.nan_to_num of the fill value outside the hull
-  const int v0 = a.vert[3 * p];
+  const int v0 = a.vert[3 * p], v1 = a.vert[3 * p + 1], v2 = a.vert[3 * p + 2];
   if (v0 >= 0) {
-    double o = 0.0;
-    o = add(o, mul(a.wgt[3 * p + 0], src[v0]));
-    o = add(o, mul(a.wgt[3 * p + 1], src[a.vert[3 * p + 1]]));
-    o = add(o, mul(a.wgt[3 * p + 2], src[a.vert[3 * p + 2]]));
-    out = isnan(o) ? 0.f : (float)o;
+    if (v0 >= a.n || v1 < 0 || v1 >= a.n || v2 < 0 || v2 >= a.n) {
+      atomicOr(a.err, 1u);  // a caller's table that does not index the coarse grid
+    } else {
+      double o = 0.0;
+      o = add(o, mul(a.wgt[3 * p + 0], src[v0]));
+      o = add(o, mul(a.wgt[3 * p + 1], src[v1]));
+      o = add(o, mul(a.wgt[3 * p + 2], src[v2]));
+      out = isnan(o) ? 0.f : (float)o;
+    }
   }
   float* dst;
   if (b == 0) dst = a.u + (int64_t)t * a.G2;
@@ -485,6 +490,9 @@ extern "C" e2e_status e2e_env_generate(const e2e_env_params* p, const int32_t* i
     return fail(E2E_ERR_INVALID, "null output array");
   const int64_t G = (int64_t)g * d, G2 = G * G;
   if (G > 46340) return fail(E2E_ERR_UNSUPPORTED, "fine grid too large");
+  if ((int64_t)nws * 2 * n > (int64_t)0x7fffffff)
+    return fail(E2E_ERR_UNSUPPORTED, "n_wsamples x 2 init_gsize^2 above 2^31 (32-bit solver dimensions)");
+  if (!(p->dxy > 0.0) || !(p->dt >= 0.0)) return fail(E2E_ERR_INVALID, "dxy must be positive and dt non-negative");
   cudaStream_t st = (cudaStream_t)stream;
   DeviceScratch scratch(st);
 
@@ -649,7 +657,11 @@ extern "C" e2e_status e2e_env_generate(const e2e_env_params* p, const int32_t* i
                                                                 phi_yi + (int64_t)t * nws * r);
     CK(cudaGetLastError());
   }
-  InterpArgs ia{nt, r, n, (int)G2, coarse, dvert, dwgt, o.u, o.v, o.phi, o.ui, o.vi, o.phi_i};
+  unsigned int* derr = nullptr;
+  CK(dalloc((void**)&derr, sizeof(unsigned int), st));
+  scratch.add(derr);
+  CK(cudaMemsetAsync(derr, 0, sizeof(unsigned int), st));
+  InterpArgs ia{nt, r, n, (int)G2, coarse, dvert, dwgt, derr, o.u, o.v, o.phi, o.ui, o.vi, o.phi_i};
   const int64_t ni = (int64_t)nt * nb * G2;
   k_env_interpolate<<<(unsigned)((ni + 255) / 256), 256, 0, st>>>(ia);
   CK(cudaGetLastError());
@@ -668,7 +680,10 @@ extern "C" e2e_status e2e_env_generate(const e2e_env_params* p, const int32_t* i
     CK(cudaMemcpyAsync(out->mask, o.mask, sizeof(int32_t) * (size_t)nt * G2, cudaMemcpyDeviceToHost, st));
   }
   if (svals_out) CK(cudaMemcpyAsync(svals_out, sv, sizeof(double) * 2 * (size_t)nt * r, cudaMemcpyDefault, st));
+  unsigned int herr = 0;
+  CK(cudaMemcpyAsync(&herr, derr, sizeof(unsigned int), cudaMemcpyDeviceToHost, st));
   CK(cudaStreamSynchronize(st));
+  if (herr) return fail(E2E_ERR_INVALID, "interpolation table: a vertex index outside the coarse grid");
   if (stats) {
     float ms = 0.f;
     CK(cudaEventElapsedTime(&ms, ev[0], ev[1]));

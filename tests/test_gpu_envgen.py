@@ -120,6 +120,31 @@ def test_randomized_svd_used_where_it_certifies(generated, name):
     assert out["stats"]["full_svds"] <= 2, out["stats"]
 
 
+def test_bad_interpolation_table_is_an_error():
+    # a caller-built table whose vertex indices leave the coarse grid: the kernel
+    # skips those reads, and the call reports E2E_ERR_INVALID
+    import ctypes as C
+
+    from e2e_gpu_dp_b200 import _lib
+    from e2e_gpu_dp_b200._lib import E2EError
+    z = _golden("env_a")
+    cfg = OE.config_from_golden(z)
+    p = envgen.env_params(**{k: v for k, v in cfg.items()})
+    vert, wgt = envgen.interp_table(cfg["init_gsize"], cfg["dxy"], cfg["interpolate_degree"])
+    inside = np.flatnonzero(vert[:, 0] >= 0)
+    vert[inside[0], 1] = cfg["init_gsize"] ** 2  # one past the last coarse cell
+    G, nt, r, nws = cfg["init_gsize"] * cfg["interpolate_degree"], cfg["nt"], cfg["n_modes"], cfg["n_wsamples"]
+    arrs = [np.empty((nt, G, G), np.float32) for _ in range(2)] + [np.empty((nt, r, G, G), np.float32) for _ in range(2)]
+    arrs += [np.empty((nt, nws, r), np.float32), np.empty((nt, G, G), np.float32), np.empty((nt, r, G, G), np.float32),
+             np.empty((nt, nws, r), np.float32), np.empty((nt, G, G), np.float32), np.empty((nt, G, G), np.int32)]
+    f = _lib.EnvFields(*[a.ctypes.data for a in arrs])
+    rc = _lib.lib().e2e_env_generate(C.byref(p), vert.ctypes.data, wgt.ctypes.data, _lib.E2E_HOST, C.byref(f),
+                                     None, None, None)
+    assert rc == _lib.E2E_ERR_INVALID
+    with pytest.raises(E2EError):
+        _lib.check(rc)
+
+
 def test_device_outputs_equal_host_outputs(generated):
     torch = pytest.importorskip("torch")
     z, cfg, out, sub = generated("env_a")
