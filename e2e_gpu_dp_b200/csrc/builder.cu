@@ -444,15 +444,55 @@ __global__ void __launch_bounds__(1024) k_build_tiles(BuildArgs A) {
   for (int base = 0; base < P.nrzns; base += kRcw) {
     const int clen = min(kRcw, P.nrzns - base);
     __syncwarp();  // previous chunk consumed
-    for (int q = a; q < clen; q += per) {
-      if (cvalid) {
-        const float* y = A.F.Y + ((int64_t)T * P.nrzns + base + q) * nm;
-        // extract_velocity, src/build_model.cu:389-401: mean + sum over modes,
-        // both sums as one chain of packed fused multiply-adds
-        float2 sum = make_float2(0.f, 0.f);
-        const float2* md = modes + cl;
+    // extract_velocity, src/build_model.cu:389-401: mean + sum over modes, both
+    // sums as one chain of packed fused multiply-adds in the reference's order
+    if (cvalid) {
+      const float2* md = modes + cl;
+      const float* yb = A.F.Y + ((int64_t)T * P.nrzns + base) * nm;
+      const int64_t ystep = (int64_t)per * nm;
+      int q = a;
+      // four of the lane's realisations at a time: each mode pair read from
+      // shared memory feeds four independent chains, and their coefficient
+      // loads are in flight together
+      for (; q + 3 * per < clen; q += 4 * per) {
+        const float* y0 = yb + (int64_t)q * nm;
+        float2 s0 = make_float2(0.f, 0.f), s1 = s0, s2 = s0, s3 = s0;
         if (y_pairs) {  // nm even, rows 8-byte aligned: coefficients two at a time
-#pragma unroll 2
+          for (int k = 0; k < nm; k += 2) {
+            const float2 m0 = md[k * 32], m1 = md[(k + 1) * 32];
+            const float2 c0 = __ldg(reinterpret_cast<const float2*>(y0 + k));
+            const float2 c1 = __ldg(reinterpret_cast<const float2*>(y0 + ystep + k));
+            const float2 c2 = __ldg(reinterpret_cast<const float2*>(y0 + 2 * ystep + k));
+            const float2 c3 = __ldg(reinterpret_cast<const float2*>(y0 + 3 * ystep + k));
+            s0 = __ffma2_rn(m0, make_float2(c0.x, c0.x), s0);
+            s1 = __ffma2_rn(m0, make_float2(c1.x, c1.x), s1);
+            s2 = __ffma2_rn(m0, make_float2(c2.x, c2.x), s2);
+            s3 = __ffma2_rn(m0, make_float2(c3.x, c3.x), s3);
+            s0 = __ffma2_rn(m1, make_float2(c0.y, c0.y), s0);
+            s1 = __ffma2_rn(m1, make_float2(c1.y, c1.y), s1);
+            s2 = __ffma2_rn(m1, make_float2(c2.y, c2.y), s2);
+            s3 = __ffma2_rn(m1, make_float2(c3.y, c3.y), s3);
+          }
+        } else {
+          for (int k = 0; k < nm; k++) {
+            const float2 m0 = md[k * 32];
+            const float c0 = __ldg(y0 + k), c1 = __ldg(y0 + ystep + k);
+            const float c2 = __ldg(y0 + 2 * ystep + k), c3 = __ldg(y0 + 3 * ystep + k);
+            s0 = __ffma2_rn(m0, make_float2(c0, c0), s0);
+            s1 = __ffma2_rn(m0, make_float2(c1, c1), s1);
+            s2 = __ffma2_rn(m0, make_float2(c2, c2), s2);
+            s3 = __ffma2_rn(m0, make_float2(c3, c3), s3);
+          }
+        }
+        myvel[q] = make_float2(u1 + s0.x, v1 + s0.y);
+        myvel[q + per] = make_float2(u1 + s1.x, v1 + s1.y);
+        myvel[q + 2 * per] = make_float2(u1 + s2.x, v1 + s2.y);
+        myvel[q + 3 * per] = make_float2(u1 + s3.x, v1 + s3.y);
+      }
+      for (; q < clen; q += per) {
+        const float* y = yb + (int64_t)q * nm;
+        float2 sum = make_float2(0.f, 0.f);
+        if (y_pairs) {
           for (int k = 0; k < nm; k += 2) {
             const float2 yy = __ldg(reinterpret_cast<const float2*>(y + k));
             sum = __ffma2_rn(md[k * 32], make_float2(yy.x, yy.x), sum);
