@@ -382,8 +382,11 @@ def run_ours(args, ws, rank, local):
     m.free()
     ro = api.rollout(prob, dev, pi, start, stream=stream)
     ro2 = api.rollout(prob, dev, pi, start, stream=stream)
+    ri = api.rollout(prob, dev, pi, start, stream=stream, interpolate=True)
     rollout = {"start": list(start), "realisations": prob.nrzns, "success_rate": ro2["stats"]["success_rate"],
-               "mean_time": ro2["stats"]["mean_time"], "kernel_s": round(ro2["stats"]["seconds"], 6)}
+               "mean_time": ro2["stats"]["mean_time"], "kernel_s": round(ro2["stats"]["seconds"], 6),
+               "interpolated": {"success_rate": ri["stats"]["success_rate"], "mean_time": ri["stats"]["mean_time"],
+                                "kernel_s": round(ri["stats"]["seconds"], 6)}}
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         from oracle import rollout as RO
         pih = pi.cpu().numpy().astype(np.int64)

@@ -106,7 +106,10 @@ class ServerStats(C.Structure):
 
 
 class RolloutOpts(C.Structure):
-    _fields_ = [("i_start", C.c_int32), ("j_start", C.c_int32), ("n_rzns", C.c_int32), ("reserved", C.c_int32)]
+    _fields_ = [("i_start", C.c_int32), ("j_start", C.c_int32), ("n_rzns", C.c_int32), ("flags", C.c_int32)]
+
+
+E2E_ROLLOUT_INTERP = 1
 
 
 class RolloutStats(C.Structure):

@@ -297,10 +297,13 @@ def build_solve(prob: Problem, fields: Dict, value=None, policy=None, stream=Non
     return V, pi, {k: getattr(st, k) for k, _ in _lib.FusedStats._fields_}
 
 
-def rollout(prob: Problem, fields: Dict, policy, start, n_rzns: int = 0, stream=None) -> Dict:
+def rollout(prob: Problem, fields: Dict, policy, start, n_rzns: int = 0, stream=None,
+            interpolate: bool = False) -> Dict:
     """Follow ``policy`` (ns int32, numpy or CUDA tensor) from ``start`` (i, j)
-    for each realisation (e2e_rollout).  Returns per-realisation arrays and
-    the summary of the reference's get_metrics."""
+    for each realisation (e2e_rollout).  ``interpolate``: actions after the
+    first interpolated from the four cells around the position (the reference
+    script's with_policy_interp).  Returns per-realisation arrays and the
+    summary of the reference's get_metrics."""
     where, f, keep = _fields_ptrs(fields)
     n = n_rzns if n_rzns > 0 else prob.nrzns
     if _is_device(policy):
@@ -313,7 +316,7 @@ def rollout(prob: Problem, fields: Dict, policy, start, n_rzns: int = 0, stream=
     tt = np.empty(n, np.int32)
     en = np.empty((n, 3), np.float32)
     fin = np.empty((n, 3), np.int32)
-    o = _lib.RolloutOpts(int(start[0]), int(start[1]), n, 0)
+    o = _lib.RolloutOpts(int(start[0]), int(start[1]), n, _lib.E2E_ROLLOUT_INTERP if interpolate else 0)
     st = _lib.RolloutStats()
     cp = c_problem(prob)
     check(lib().e2e_rollout(C.byref(cp), C.byref(f), where, pptr, pw, C.byref(o), succ.ctypes.data,

@@ -17,6 +17,20 @@
 // chosen order is the velocity dot product u + sum_k ui_k * Y_k: a sequential
 // fma chain over the modes (the reference's np.matmul leaves that order to
 // its BLAS library).
+//
+// With interp set, the actions after the first are interpolated from the
+// policy of the four cells around the vehicle's position (the script's
+// with_policy_interp branch: get_interpolated_action :174-198,
+// interpolate_action_angles :111-171, bilinear / triangle interpolation
+// :37-108) in the types NumPy gives them: the bilinear form in float32 with
+// its two small matrix products as separately rounded products summed in
+// order (NumPy's float32 matmul of these shapes, checked on the host), the
+// triangle form (next to the target cell) with float64 weights, after which
+// the reference's position is float64 and this kernel's movement continues in
+// double.  Heading atan2, its cosine and the speed's square root are CUDA's;
+// the reference takes them from the host libm and NumPy's scalar power, which
+// can differ in the last bit, so interpolated trajectories agree with the
+// reference's per realisation almost always rather than bit for bit.
 #include <cuda_runtime.h>
 
 #include <cmath>
@@ -45,6 +59,7 @@ struct RolloutArgs {
   const float* cosv;   // na
   const float* sinv;   // na
   int g, nt, nm, na, tsg, it, jt, i0, j0, nrzns, nrzns_field;
+  int interp;          // actions after the first interpolated from the policy
   float dt, dj, di;
   int8_t* success;     // per realisation: 1 target, 0 failed, -1 undecided, -2 invalid policy entry
   int32_t* ttime;
@@ -76,6 +91,140 @@ __device__ __forceinline__ float divmod32(float a, float b, float& rem) {
   return fl;
 }
 
+// NumPy's float64 divmod (the same algorithm as divmod32, in double)
+__device__ __forceinline__ double divmod64(double a, double b, double& rem) {
+  double mod = fmod(a, b);
+  double div = (a - mod) / b;
+  if (mod != 0.0) {
+    if ((b < 0.0) != (mod < 0.0)) {
+      mod += b;
+      div -= 1.0;
+    }
+  } else {
+    mod = copysign(0.0, b);
+  }
+  double fl;
+  if (div != 0.0) {
+    fl = floor(div);
+    if (div - fl > 0.5) fl += 1.0;
+  } else {
+    fl = copysign(0.0, a / b);
+  }
+  rem = mod;
+  return fl;
+}
+
+// Python's float % with a positive modulus (CPython float_rem)
+__device__ __forceinline__ double py_mod(double a, double b) {
+  double m = fmod(a, b);
+  if (m != 0.0) {
+    if ((b < 0.0) != (m < 0.0)) m += b;
+  } else {
+    m = copysign(0.0, b);
+  }
+  return m;
+}
+
+// The interpolated action at (x, y) in cell (t, i, j): speed (float32, or
+// double in *speed_d with *wide_out set when the triangle form ran or the
+// position was already double) and heading in [0, 2pi).
+struct Interp {
+  float speed;
+  double speed_d, angle;
+  bool wide;
+  bool bad;  // a support cell's policy entry is not an action (the reference's lookup fails there)
+};
+
+__device__ Interp interp_action(const RolloutArgs& A, int t, int i, int j, float xf, float yf, double xd, double yd,
+                                bool wide) {
+  const int g = A.g;
+  const int64_t nc = (int64_t)g * g;
+  const double x = wide ? xd : (double)xf, y = wide ? yd : (double)yf;
+  const int fx = (x - (double)A.xs[j] < 0.0) ? -1 : 1;  // f(delx), the sign of an exact difference
+  const int fy = (y - (double)A.ys[g - 1 - i] < 0.0) ? -1 : 1;
+  const int si[4] = {i, i - fy, i, i - fy}, sj[4] = {j, j, j + fx, j + fx};
+  int term[4];
+  float vx[4], vy[4];
+  Interp r;
+  r.bad = false;
+  for (int k = 0; k < 4; ++k) {
+    term[k] = (si[k] == A.it && sj[k] == A.jt) ? 1 : 0;
+    const int a = A.policy[(int64_t)t * nc + (int64_t)si[k] * g + sj[k]];
+    if (a < 0 || a >= A.na) r.bad = true;
+    const int aa = r.bad ? 0 : a;
+    vx[k] = __fmul_rn(A.speed[aa], A.cosv[aa]);
+    vy[k] = __fmul_rn(A.speed[aa], A.sinv[aa]);
+  }
+  bool tri = false;
+  if (term[0] == 0 && term[1] == 0 && term[2] == 1) {  // [0,0,1,1] / [0,0,1,0]
+    vx[2] = vx[0];
+    vx[3] = vx[1];
+    vy[2] = vy[0];
+    vy[3] = vy[1];
+  } else if (term[0] == 0 && term[1] == 1 && term[2] == 0) {  // [0,1,0,1] / [0,1,0,0]
+    vx[1] = vx[0];
+    vx[3] = vx[2];
+    vy[1] = vy[0];
+    vy[3] = vy[2];
+  } else if (term[0] == 0 && term[1] == 0 && term[2] == 0 && term[3] == 1) {
+    tri = true;
+  }
+  const float x1 = A.xs[j], x2 = A.xs[j + fx];
+  const float y1 = A.ys[g - 1 - i], y2 = A.ys[g - 1 - (i - fy)];
+  double ivx, ivy;
+  if (!tri && !wide) {  // float32: denom * (x_vec @ (val_mat @ y_vec))
+    const float den = __fdiv_rn(1.0f, __fmul_rn(__fsub_rn(x2, x1), __fsub_rn(y2, y1)));
+    const float xa = __fsub_rn(x2, xf), xb = __fsub_rn(xf, x1);
+    const float ya = __fsub_rn(y2, yf), yb = __fsub_rn(yf, y1);
+    auto bil = [&](const float* v) {
+      const float in0 = __fadd_rn(__fmul_rn(v[0], ya), __fmul_rn(v[1], yb));
+      const float in1 = __fadd_rn(__fmul_rn(v[2], ya), __fmul_rn(v[3], yb));
+      return __fmul_rn(den, __fadd_rn(__fmul_rn(xa, in0), __fmul_rn(xb, in1)));
+    };
+    const float fvx = bil(vx), fvy = bil(vy);
+    r.angle = py_mod(atan2((double)fvy, (double)fvx) + 2.0 * M_PI, 2.0 * M_PI);
+    r.speed = sqrtf(__fadd_rn(__fmul_rn(fvx, fvx), __fmul_rn(fvy, fvy)));
+    r.speed_d = r.speed;
+    r.wide = false;
+    return r;
+  }
+  if (!tri) {  // position already double: the same form promoted to float64
+    const double den = (double)__fdiv_rn(1.0f, __fmul_rn(__fsub_rn(x2, x1), __fsub_rn(y2, y1)));
+    const double xa = (double)x2 - x, xb = x - (double)x1, ya = (double)y2 - y, yb = y - (double)y1;
+    auto bil = [&](const float* v) {
+      const double in0 = __dadd_rn(__dmul_rn(v[0], ya), __dmul_rn(v[1], yb));
+      const double in1 = __dadd_rn(__dmul_rn(v[2], ya), __dmul_rn(v[3], yb));
+      return __dmul_rn(den, __dadd_rn(__dmul_rn(xa, in0), __dmul_rn(xb, in1)));
+    };
+    ivx = bil(vx);
+    ivy = bil(vy);
+  } else {  // triangle through (x1, y1), (x1, y2), (x2, y1); weights float32 (double once wide), then float64
+    const float d23y = __fsub_rn(y2, y1), d13x = __fsub_rn(x1, x2), d32x = __fsub_rn(x2, x1);
+    const float d0y = __fsub_rn(y1, y1);  // b1 - b3 and b3 - b1 of the reference's expressions
+    const double den = __fadd_rn(__fmul_rn(d23y, d13x), __fmul_rn(d32x, d0y));
+    double w0, w1;
+    if (!wide) {
+      const float xa3 = __fsub_rn(xf, x2), yb3 = __fsub_rn(yf, y1);
+      w0 = __fadd_rn(__fmul_rn(d23y, xa3), __fmul_rn(d32x, yb3));
+      w1 = __fadd_rn(__fmul_rn(d0y, xa3), __fmul_rn(d13x, yb3));
+    } else {
+      const double xa3 = x - (double)x2, yb3 = y - (double)y1;
+      w0 = __dadd_rn(__dmul_rn(d23y, xa3), __dmul_rn(d32x, yb3));
+      w1 = __dadd_rn(__dmul_rn(d0y, xa3), __dmul_rn(d13x, yb3));
+    }
+    w0 = w0 / den;
+    w1 = w1 / den;
+    const double w2 = (1.0 - w0) - w1;
+    ivx = __dadd_rn(__dadd_rn(__dmul_rn(vx[0], w0), __dmul_rn(vx[1], w1)), __dmul_rn(vx[2], w2));
+    ivy = __dadd_rn(__dadd_rn(__dmul_rn(vy[0], w0), __dmul_rn(vy[1], w1)), __dmul_rn(vy[2], w2));
+  }
+  r.angle = py_mod(atan2(ivy, ivx) + 2.0 * M_PI, 2.0 * M_PI);
+  r.speed_d = sqrt(__dadd_rn(__dmul_rn(ivx, ivx), __dmul_rn(ivy, ivy)));
+  r.speed = (float)r.speed_d;
+  r.wide = true;
+  return r;
+}
+
 __global__ void __launch_bounds__(128) k_rollout(RolloutArgs A) {
   const int rzn = blockIdx.x * blockDim.x + threadIdx.x;
   if (rzn >= A.nrzns) return;
@@ -84,14 +233,26 @@ __global__ void __launch_bounds__(128) k_rollout(RolloutArgs A) {
   auto term = [&](int i, int j) { return i >= A.it && i < A.it + A.tsg && j >= A.jt && j < A.jt + A.tsg; };
   int t = 0, i = A.i0, j = A.j0;
   float x = A.xs[j], y = A.ys[g - 1 - i];
+  double xd = 0.0, yd = 0.0;  // the position once it is float64 (after a triangle-form action)
+  bool wide = false;
+  // the action: speed and heading cosine / sine (float32), or in double for a
+  // float64 interpolated action
+  bool act_d = false;
+  float thr = 0.f, cth = 0.f, sth = 0.f;
+  double thr_d = 0.0, cth_d = 0.0, sth_d = 0.0;
   const float xs0 = A.xs[0], xsn = A.xs[g - 1], ys0 = A.ys[0], ysn = A.ys[g - 1];
   int a = A.policy[(int64_t)t * nc + (int64_t)i * g + j];
+  if (a >= 0 && a < A.na) {
+    thr = A.speed[a];
+    cth = A.cosv[a];
+    sth = A.sinv[a];
+  }
   int success = -1;  // -1: undecided (the reference's None)
   float e_cons = 0.f, e_col = 0.f, e_net = 0.f;
   int travel = 0;
   for (int it = 0; it < nt; ++it) {
     if (success == -1) {
-      if (a < 0 || a >= A.na) {  // the reference indexes its action list with it and fails
+      if (!act_d && (a < 0 || a >= A.na)) {  // the reference indexes its action list with it and fails
         success = -2;
         break;
       }
@@ -106,10 +267,10 @@ __global__ void __launch_bounds__(128) k_rollout(RolloutArgs A) {
       const float vx = __fadd_rn(A.F.u[cell], dx_);
       const float vy = __fadd_rn(A.F.v[cell], dy_);
       const float rad1 = A.F.s[cell];
-      if (!term(i, j) && t < nt - 1) {  // move_exact
-        const float thrust = A.speed[a];
-        const float vnx = __fadd_rn(__fmul_rn(thrust, A.cosv[a]), vx);
-        const float vny = __fadd_rn(__fmul_rn(thrust, A.sinv[a]), vy);
+      if (!term(i, j) && t < nt - 1 && !act_d) {  // move_exact
+        const float thrust = thr;
+        const float vnx = __fadd_rn(__fmul_rn(thrust, cth), vx);
+        const float vny = __fadd_rn(__fmul_rn(thrust, sth), vy);
         float xn = __fadd_rn(x, __fmul_rn(vnx, A.dt));
         float yn = __fadd_rn(y, __fmul_rn(vny, A.dt));
         if (xn > xsn) xn = xsn;
@@ -128,10 +289,34 @@ __global__ void __launch_bounds__(128) k_rollout(RolloutArgs A) {
           j = (int)xind;
         }
         t += 1;
+      } else if (!term(i, j) && t < nt - 1) {  // move_exact with a float64 action: the position becomes float64
+        const double vnx = __dadd_rn(__dmul_rn(thr_d, cth_d), (double)vx);
+        const double vny = __dadd_rn(__dmul_rn(thr_d, sth_d), (double)vy);
+        double xn = __dadd_rn(wide ? xd : (double)x, __dmul_rn(vnx, (double)A.dt));
+        double yn = __dadd_rn(wide ? yd : (double)y, __dmul_rn(vny, (double)A.dt));
+        if (xn > xsn) xn = xsn;
+        else if (xn < xs0) xn = xs0;
+        if (yn > ysn) yn = ysn;
+        else if (yn < ys0) yn = ys0;
+        xd = xn;
+        yd = yn;
+        x = (float)xn;
+        y = (float)yn;
+        wide = true;
+        double remx, remy;
+        double xind = divmod64(xn - (double)xs0, (double)A.dj, remx);
+        double yind = divmod64(-(yn - (double)ysn), (double)A.di, remy);
+        if (remx >= (double)__fmul_rn(0.5f, A.dj)) xind += 1.0;
+        if (remy >= (double)__fmul_rn(0.5f, A.di)) yind += 1.0;
+        if (!(isnan(xind) || isnan(yind))) {
+          i = (int)yind;
+          j = (int)xind;
+        }
+        t += 1;
       }
       const float rad2 = A.F.s[(int64_t)t * nc + (int64_t)i * g + j];
       travel += 1;
-      const float sp = A.speed[a];
+      const float sp = act_d ? (float)thr_d : thr;
       const float sp2 = __fmul_rn(sp, sp);
       const float half = __fdiv_rn(__fadd_rn(rad2, rad1), 2.0f);
       e_cons = __fadd_rn(e_cons, sp2);
@@ -140,7 +325,29 @@ __global__ void __launch_bounds__(128) k_rollout(RolloutArgs A) {
     }
     if (i == 0 || i == g - 1 || j == 0 || j == g - 1 || A.F.mask[(int64_t)t * nc + (int64_t)i * g + j] == 1)
       success = 0;
-    if (!term(i, j) && t < nt - 1 && success == -1) a = A.policy[(int64_t)t * nc + (int64_t)i * g + j];
+    if (!term(i, j) && t < nt - 1 && success == -1) {
+      if (A.interp) {
+        const Interp r = interp_action(A, t, i, j, x, y, xd, yd, wide);
+        if (r.bad) {
+          success = -2;
+          break;
+        }
+        act_d = r.wide;
+        thr = r.speed;
+        thr_d = r.speed_d;
+        cth = (float)cos(r.angle);
+        sth = (float)sin(r.angle);
+        cth_d = cos(r.angle);
+        sth_d = sin(r.angle);
+      } else {
+        a = A.policy[(int64_t)t * nc + (int64_t)i * g + j];
+        if (a >= 0 && a < A.na) {
+          thr = A.speed[a];
+          cth = A.cosv[a];
+          sth = A.sinv[a];
+        }
+      }
+    }
     else if (term(i, j)) success = 1;
     else success = 0;
   }
@@ -251,6 +458,7 @@ extern "C" e2e_status e2e_rollout(const e2e_problem* p, const e2e_fields* f, int
   A.nrzns = n;
   A.nrzns_field = p->nrzns;
   A.dt = p->dt;
+  A.interp = (opts->flags & E2E_ROLLOUT_INTERP) ? 1 : 0;
   A.dj = std::fabs(tab[1] - tab[0]);
   A.di = std::fabs(tab[g + 1] - tab[g]);
   A.success = d_succ;

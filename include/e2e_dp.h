@@ -321,10 +321,13 @@ e2e_status e2e_server_destroy(e2e_server* s);
  * the target (terminal subgrid of p), an edge or obstacle cell, or the last
  * step.  Float32 arithmetic as the reference under NumPy's scalar rules; the
  * mode sum of the velocity is a sequential fma chain. */
+enum { E2E_ROLLOUT_INTERP = 1 };
 typedef struct {
   int32_t i_start, j_start; /* start cell at t = 0 */
   int32_t n_rzns;           /* realisations to follow (0 = all of the field's) */
-  int32_t reserved;
+  int32_t flags;            /* E2E_ROLLOUT_INTERP: actions after the first interpolated from the policy of
+                               the four cells around the position (the script's with_policy_interp,
+                               Post_processing/plot_e2eGPU_policy.py:174-198); 0: the cell's own action */
 } e2e_rollout_opts;
 
 typedef struct {

@@ -19,6 +19,15 @@ scalar stays float32).  The velocity of a realisation at a cell is
 Per realisation: outcome (1 reached the target, 0 failed, -1 never decided),
 travel time (steps), energy terms (sum F^2, sum of mean scalar field, their
 difference) and the final (t, i, j).
+
+``interp=True`` restates the script's ``with_policy_interp`` branch
+(plot_e2eGPU_policy.py:483-486, get_interpolated_action :174-198,
+interpolate_action_angles :111-171, bilinear / triangle interpolation
+:37-108): after the first step the action is interpolated from the policy of
+the four cells around the vehicle's position, in the same NumPy expressions
+(float32 small matrix products, a float64 weight vector for the triangle case,
+NumPy scalar powers); pinned against tests/golden/rollout_interp_*.npz, which
+the reference's own functions produced.
 """
 import math
 from typing import Dict, Tuple
@@ -70,7 +79,69 @@ def _divmod32(a, b):
     return fl, mod
 
 
-def rollout(prob, fields: Dict[str, np.ndarray], policy: np.ndarray, start, n_rzns=None, dot="fma"):
+def _bilinear(x, y, xt, yt, vals):
+    v11, v12, v21, v22 = vals
+    x1, x2 = xt
+    y1, y2 = yt
+    denom = 1 / ((x2 - x1) * (y2 - y1))
+    xv = np.array([x2 - x, x - x1]).reshape((1, 2))
+    vm = np.array([[v11, v12], [v21, v22]])
+    yv = np.array([y2 - y, y - y1]).reshape((2, 1))
+    return (denom * np.matmul(xv, np.matmul(vm, yv)))[0][0]
+
+
+def _triangle(x, y, pts, vals):
+    (x1, y1), (x2, y2), (x3, y3) = pts
+    V = np.array(vals)
+    W = np.zeros((3,))
+    den = (y2 - y3) * (x1 - x3) + (x3 - x2) * (y1 - y3)
+    W[0] = (y2 - y3) * (x - x3) + (x3 - x2) * (y - y3)
+    W[1] = (y3 - y1) * (x - x3) + (x1 - x3) * (y - y3)
+    W[0] = W[0] / den
+    W[1] = W[1] / den
+    W[2] = 1 - W[0] - W[1]
+    return np.dot(V, W)
+
+
+def interp_action(pol, speeds, angles, xs, ys, g, t, i, j, x, y, endpos):
+    """(speed, heading) interpolated from the policy of the cell (t, i, j) that
+    holds (x, y) and its three neighbours towards (x, y)."""
+    sgn = lambda d: -1 if d < 0 else 1  # noqa: E731
+    dy_, dx_ = sgn(y - ys[g - 1 - i]), sgn(x - xs[j])
+    sup = [(t, i, j), (t, i - dy_, j), (t, i, j + dx_), (t, i - dy_, j + dx_)]
+    term = [1 if (si, sj) == endpos else 0 for (_, si, sj) in sup]
+    acts = [int(pol[sj + g * si + g * g * st]) for (st, si, sj) in sup]
+    F = [speeds[a] for a in acts]
+    th = [angles[a] for a in acts]
+    cx = [xs[sj] for (_, _, sj) in sup]
+    cy = [ys[g - 1 - si] for (_, si, _) in sup]
+    vx = [F[k] * math.cos(th[k]) for k in range(4)]
+    vy = [F[k] * math.sin(th[k]) for k in range(4)]
+    method = "bilinear"
+    if term == [0, 0, 0, 0]:
+        pass
+    elif term in ([0, 0, 1, 1], [0, 0, 1, 0]):
+        vx[2], vx[3], vy[2], vy[3] = vx[0], vx[1], vy[0], vy[1]
+    elif term in ([0, 1, 0, 1], [0, 1, 0, 0]):
+        vx[1], vx[3], vy[1], vy[3] = vx[0], vx[2], vy[0], vy[2]
+    elif term == [0, 0, 0, 1]:
+        method = "triangle"
+    else:
+        raise ValueError(f"terminal pattern {term} cannot occur")
+    x1, y1, x2, y2 = cx[0], cy[0], cx[3], cy[3]
+    if method == "bilinear":
+        ivx = _bilinear(x, y, (x1, x2), (y1, y2), vx)
+        ivy = _bilinear(x, y, (x1, x2), (y1, y2), vy)
+    else:
+        pts = [(x1, y1), (x1, y2), (x2, y1)]
+        ivx = _triangle(x, y, pts, [vx[0], vx[1], vx[2]])
+        ivy = _triangle(x, y, pts, [vy[0], vy[1], vy[2]])
+    ang = (math.atan2(ivy, ivx) + 2 * np.pi) % (2 * np.pi)
+    return (ivx ** 2 + ivy ** 2) ** 0.5, ang
+
+
+def rollout(prob, fields: Dict[str, np.ndarray], policy: np.ndarray, start, n_rzns=None, dot="fma",
+            interp=False):
     params = prob.prob_params()
     g, nt = int(params[0]), int(params[10])
     dx, dy, dt = params[16], params[17], params[4]
@@ -102,6 +173,7 @@ def rollout(prob, fields: Dict[str, np.ndarray], policy: np.ndarray, start, n_rz
         t, i, j = 0, int(start[0]), int(start[1])
         x, y = xs[j], ys[g - 1 - i]
         a = int(pol[j + g * i + g * g * t])
+        act = (speeds[a], angles[a])
         success = None
         e_cons = e_col = e_net = 0
         travel = 0
@@ -110,7 +182,7 @@ def rollout(prob, fields: Dict[str, np.ndarray], policy: np.ndarray, start, n_rz
                 vx, vy = vel(t, i, j, rzn)
                 rad1 = s_mat[t, i, j]
                 if not term(i, j) and t < nt - 1:          # move_exact (:162-269)
-                    thrust, angle = speeds[a], angles[a]
+                    thrust, angle = act
                     vnx = (thrust * math.cos(angle)) + vx
                     vny = (thrust * math.sin(angle)) + vy
                     xn = x + (vnx * dt)
@@ -135,13 +207,17 @@ def rollout(prob, fields: Dict[str, np.ndarray], policy: np.ndarray, start, n_rz
                     t += 1
                 rad2 = s_mat[t, i, j]
                 travel += 1
-                e_cons += (1 * speeds[a]) ** 2
+                e_cons += (1 * act[0]) ** 2
                 e_col += (1 * (rad2 + rad1) / 2)
-                e_net += (1 * (speeds[a] ** 2)) - (1 * (rad2 + rad1) / 2)
+                e_net += (1 * (act[0] ** 2)) - (1 * (rad2 + rad1) / 2)
             if i == 0 or i == g - 1 or j == 0 or j == g - 1 or mask[t, i, j] == 1:
                 success = False
             if (not term(i, j)) and t < nt - 1 and success is None:
-                a = int(pol[j + g * i + g * g * t])
+                if interp:
+                    act = interp_action(pol, speeds, angles, xs, ys, g, t, i, j, x, y, (it, jt))
+                else:
+                    a = int(pol[j + g * i + g * g * t])
+                    act = (speeds[a], angles[a])
             elif term(i, j):
                 success = True
             else:

@@ -42,3 +42,17 @@ def test_oracle_reproduces_reference_trajectories(name, dot):
             assert np.array_equal(r[e], fx[f"{e}_{k}"])
     m = RO.metrics(r)
     assert 0.0 <= m["success_rate"] <= 1.0
+
+
+@pytest.mark.parametrize("name", NAMES)
+def test_oracle_interpolated_policy_reproduces_reference(name):
+    # tests/golden/rollout_interp_<name>.npz: the reference's get_interpolated_action
+    # (with_policy_interp) after the first step; the restatement uses the same
+    # NumPy expressions, so with NumPy's dot product it agrees bit for bit
+    prob, fields = problem(name)
+    pol = golden(name)["policy"].astype(np.int64)
+    fx = np.load(os.path.join(os.path.dirname(__file__), "golden", f"rollout_interp_{name}.npz"))
+    for k, st in enumerate(fx["starts"]):
+        r = RO.rollout(prob, fields, pol, st, dot="numpy", interp=True)
+        for key in ("success", "travel_time", "final_tij", "energy_cons", "energy_col", "net_energy"):
+            assert np.array_equal(r[key], fx[f"{key}_{k}"]), (name, k, key)
