@@ -515,7 +515,7 @@ __global__ void __launch_bounds__(1024) k_build_tiles(BuildArgs A) {
       if (plain_warp) {
         // counts only: the rewards are folded from the counters at the end, a
         // sample that leaves the window counts in the miss bin
-#pragma unroll 8
+#pragma unroll 16
         for (int q = 0; q < clen; ++q) {
           const float2 vv = myvel[q];
           const float2 xy = advect2(FF, csn, vv, dt2, xy1);  // move(), src/build_model.cu:284-289
@@ -539,7 +539,7 @@ __global__ void __launch_bounds__(1024) k_build_tiles(BuildArgs A) {
         const uint64_t m_edge = masks[MASK_EDGE * nthr + tid];
         const uint64_t m_term = masks[MASK_TERM * nthr + tid];
         const uint64_t m_slow = masks[MASK_SLOW * nthr + tid];
-#pragma unroll 4
+#pragma unroll 8
         for (int q = 0; q < clen; ++q) {
           const float2 vv = myvel[q];
           const float2 xy = advect2(FF, csn, vv, dt2, xy1);
