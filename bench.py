@@ -21,6 +21,7 @@ import argparse
 import gc
 import json
 import os
+import resource
 import statistics
 import subprocess
 import sys
@@ -273,13 +274,18 @@ def run_ours(args, ws, rank, local):
     pi = torch.empty(prob.ns, dtype=torch.int32, device="cuda")
 
     def step(record=None):
+        r0 = resource.getrusage(resource.RUSAGE_SELF)
         t0 = time.perf_counter()
         m = api.build_model(prob, dev, stream=stream)
         t1 = time.perf_counter()
         _, _, st = m.solve(method="layered", value=V, policy=pi, stream=stream)
         t2 = time.perf_counter()
         if record is not None:
-            record.append((m.info(), st, (round((t1 - t0) * 1e3, 1), round((t2 - t1) * 1e3, 1))))
+            r1 = resource.getrusage(resource.RUSAGE_SELF)
+            host = {"cpu_ms": round((r1.ru_utime + r1.ru_stime - r0.ru_utime - r0.ru_stime) * 1e3, 1),
+                    "involuntary_switches": r1.ru_nivcsw - r0.ru_nivcsw,
+                    "page_faults": r1.ru_minflt - r0.ru_minflt + r1.ru_majflt - r0.ru_majflt}
+            record.append((m.info(), st, (round((t1 - t0) * 1e3, 1), round((t2 - t1) * 1e3, 1)), host))
         m.free()
 
     recs = []
@@ -456,6 +462,8 @@ def run_ours(args, ws, rank, local):
                 "step_build_solve_wall_ms": e2e_split},
         "gpu_launches": launches,
         "step_ms": step_ms, "step_host_ms": [r[2] for r in recs],
+        # the calling process per step: CPU time, preemptions, page faults
+        "step_host_usage": [r[3] for r in recs],
         "step_phases_ms": [{"build_kernel": round(r[0]["build_kernel_ms"], 2), "assemble": round(r[0]["assemble_ms"], 2),
                             "pack": round(r[1]["pack_ms"], 2), "solve": round(r[1]["seconds"] * 1e3, 2)}
                            for r in recs],
@@ -898,7 +906,8 @@ def profile_batch():
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--steps", type=int, default=None,
+                    help="timed steps (default 10; the reference arm, 42 s a step, 3)")
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -930,6 +939,8 @@ def main():
         print(json.dumps({"envgen": run_envgen()}), flush=True)
         return 0
     ws, rank, local = _dist()
+    if args.steps is None:
+        args.steps = 3 if args.impl == "reference" else 10
     if args.impl == "reference":
         out = run_reference(args, ws, rank, local)
         if out is not None:

@@ -1,13 +1,16 @@
 // Host orchestration and the C ABI declared in include/e2e_dp.h.
 #include <cuda_runtime.h>
+#include <sys/resource.h>
 
 #include <algorithm>
 #include <chrono>
+#include <cstdlib>
 #include <mutex>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
 #include <string>
+#include <unordered_map>
 #include <vector>
 
 #include "e2e_dp.h"
@@ -75,11 +78,254 @@ cudaError_t device_pool(cudaMemPool_t* out) {
   return cudaSuccess;
 }
 
+}  // namespace e2e
+
+// ---------------------------------------------------------------------------------
+// large-block cache.  Blocks of 8 MiB and more that the library frees are kept,
+// with an event recorded on the freeing stream, and handed to the next request
+// of about the same size (at most a quarter larger) after a stream wait on that
+// event.  Repeated builds and solves then take no pool allocation at all: the
+// pool serves them from its reserve too, but a request that its free ranges do
+// not fit as they lie goes through the driver, which on a busy machine took from
+// a few to several hundred milliseconds.  Bounded per device (a quarter of its
+// memory, oldest blocks returned first); a failed pool allocation empties it and
+// retries; e2e_memory_trim empties it.
+// ---------------------------------------------------------------------------------
+namespace {
+constexpr size_t kCacheMinBytes = size_t(8) << 20;
+
+struct CachedBlock {
+  void* p;
+  size_t bytes;
+  cudaEvent_t ev;  // recorded on the freeing stream
+  uint64_t seq;
+};
+
+struct BlockCache {
+  std::mutex mu;
+  std::vector<CachedBlock> free;
+  std::vector<cudaEvent_t> spare_events;
+  size_t free_bytes = 0, cap = 0;
+  uint64_t seq = 0;
+};
+BlockCache g_cache[64];
+// large blocks handed out, of every device (device pointers are unique): size and device
+std::mutex g_live_mu;
+std::unordered_map<void*, std::pair<size_t, int>> g_live;
+
+int current_device() {
+  int dev = -1;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return -1;
+  return dev;
+}
+
+// every cached block of the device, released on stream st once its free is done
+void drop_cached(int dev, cudaStream_t st) {
+  BlockCache& c = g_cache[dev];
+  std::vector<CachedBlock> v;
+  {
+    std::lock_guard<std::mutex> lk(c.mu);
+    v.swap(c.free);
+    c.free_bytes = 0;
+  }
+  for (CachedBlock& b : v) {
+    cudaStreamWaitEvent(st, b.ev, 0);
+    cudaEventDestroy(b.ev);
+    cudaFreeAsync(b.p, st);
+  }
+}
+}  // namespace
+
+namespace e2e {
 cudaError_t dalloc(void** p, size_t bytes, cudaStream_t st) {
   cudaMemPool_t pool;
   cudaError_t e = device_pool(&pool);
   if (e != cudaSuccess) return e;
-  return cudaMallocFromPoolAsync(p, bytes ? bytes : 16, pool, st);
+  if (bytes < kCacheMinBytes) return cudaMallocFromPoolAsync(p, bytes ? bytes : 16, pool, st);
+  const int dev = current_device();
+  if (dev < 0) return cudaErrorInvalidDevice;
+  BlockCache& c = g_cache[dev];
+  CachedBlock got{nullptr, 0, nullptr, 0};
+  {
+    std::lock_guard<std::mutex> lk(c.mu);
+    int best = -1;
+    for (int i = 0; i < (int)c.free.size(); ++i) {
+      const CachedBlock& b = c.free[i];
+      if (b.bytes < bytes || b.bytes > bytes + bytes / 4) continue;
+      if (best < 0 || b.bytes < c.free[best].bytes ||
+          (b.bytes == c.free[best].bytes && b.seq > c.free[best].seq))
+        best = i;
+    }
+    if (best >= 0) {
+      got = c.free[best];
+      c.free.erase(c.free.begin() + best);
+      c.free_bytes -= got.bytes;
+    }
+  }
+  if (got.p) {
+    {
+      std::lock_guard<std::mutex> lk(g_live_mu);
+      g_live[got.p] = {got.bytes, dev};
+    }
+    e = cudaStreamWaitEvent(st, got.ev, 0);
+    {
+      std::lock_guard<std::mutex> lk(c.mu);
+      c.spare_events.push_back(got.ev);
+    }
+    if (e != cudaSuccess) {
+      dfree(got.p, st);
+      return e;
+    }
+    *p = got.p;
+    return cudaSuccess;
+  }
+  e = cudaMallocFromPoolAsync(p, bytes, pool, st);
+  if (e == cudaErrorMemoryAllocation) {
+    cudaGetLastError();
+    drop_cached(dev, st);
+    e = cudaMallocFromPoolAsync(p, bytes, pool, st);
+  }
+  if (e != cudaSuccess) return e;
+  std::lock_guard<std::mutex> lk(g_live_mu);
+  g_live[*p] = {bytes, dev};
+  return cudaSuccess;
+}
+
+void dfree(void* p, cudaStream_t st) {
+  if (!p) return;
+  const int dev = current_device();
+  size_t bytes = 0;
+  {
+    std::lock_guard<std::mutex> lk(g_live_mu);
+    auto it = g_live.find(p);
+    if (it != g_live.end()) {
+      if (it->second.second == dev) bytes = it->second.first;
+      g_live.erase(it);
+    }
+  }
+  if (!bytes) {  // a small block, or one freed with another device current: to the pool
+    cudaFreeAsync(p, st);
+    return;
+  }
+  BlockCache* c = &g_cache[dev];
+  cudaEvent_t ev = nullptr;
+  {
+    std::lock_guard<std::mutex> lk(c->mu);
+    if (!c->spare_events.empty()) {
+      ev = c->spare_events.back();
+      c->spare_events.pop_back();
+    }
+  }
+  if (!ev && cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) != cudaSuccess) ev = nullptr;
+  if (!ev || cudaEventRecord(ev, st) != cudaSuccess) {
+    if (ev) cudaEventDestroy(ev);
+    cudaFreeAsync(p, st);
+    return;
+  }
+  std::vector<CachedBlock> evict;
+  {
+    std::lock_guard<std::mutex> lk(c->mu);
+    if (!c->cap) {
+      size_t fr = 0, total = 0;
+      c->cap = cudaMemGetInfo(&fr, &total) == cudaSuccess ? total / 4 : (size_t(16) << 30);
+    }
+    c->free.push_back({p, bytes, ev, ++c->seq});
+    c->free_bytes += bytes;
+    while (c->free_bytes > c->cap && !c->free.empty()) {
+      auto old = std::min_element(c->free.begin(), c->free.end(),
+                                  [](const CachedBlock& a, const CachedBlock& b) { return a.seq < b.seq; });
+      c->free_bytes -= old->bytes;
+      evict.push_back(*old);
+      c->free.erase(old);
+    }
+  }
+  for (CachedBlock& b : evict) {
+    cudaStreamWaitEvent(st, b.ev, 0);
+    cudaEventDestroy(b.ev);
+    cudaFreeAsync(b.p, st);
+  }
+}
+
+// A stream synchronisation spins the calling thread for the whole wait (0.44 s
+// of CPU per 200x200x120 build); a blocking-sync event lets it sleep and be
+// woken by the device, so a busy host does not hold up the next launch.
+cudaError_t sleep_sync(cudaStream_t st) {
+  cudaEvent_t ev;
+  cudaError_t e = cudaEventCreateWithFlags(&ev, cudaEventBlockingSync | cudaEventDisableTiming);
+  if (e != cudaSuccess) return e;
+  e = cudaEventRecord(ev, st);
+  if (e == cudaSuccess) e = cudaEventSynchronize(ev);
+  cudaError_t d = cudaEventDestroy(ev);
+  return e != cudaSuccess ? e : d;
+}
+}  // namespace e2e
+
+namespace {
+thread_local e2e::HostTrace* g_trace = nullptr;
+
+bool trace_enabled() {
+  static const bool on = [] {
+    const char* v = std::getenv("E2E_TRACE");
+    return v && v[0] && v[0] != '0';
+  }();
+  return on;
+}
+
+double now_ms() {
+  return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+
+void usage(double* cpu_ms, long* nv, long* niv) {
+  rusage r;
+  getrusage(RUSAGE_THREAD, &r);
+  *cpu_ms = (r.ru_utime.tv_sec + r.ru_stime.tv_sec) * 1e3 + (r.ru_utime.tv_usec + r.ru_stime.tv_usec) * 1e-3;
+  *nv = r.ru_nvcsw;
+  *niv = r.ru_nivcsw;
+}
+}  // namespace
+
+namespace e2e {
+HostTrace::HostTrace(const char* nm) : name(nm) {
+  if (!trace_enabled()) return;
+  on = true;
+  cudaMemPool_t pool;
+  uint64_t r = 0;
+  if (device_pool(&pool) == cudaSuccess && cudaMemPoolGetAttribute(pool, cudaMemPoolAttrReservedMemCurrent, &r) == cudaSuccess)
+    pool0 = r;
+  t0 = last = now_ms();
+  usage(&cpu0, &nv0, &niv0);
+  prev = g_trace;
+  g_trace = this;
+}
+
+void HostTrace::mark(const char* what) {
+  if (!on) return;
+  const double t = now_ms();
+  char b[96];
+  std::snprintf(b, sizeof(b), " %s=%.2f", what, t - last);
+  line += b;
+  last = t;
+}
+
+HostTrace::~HostTrace() {
+  if (!on) return;
+  g_trace = prev;
+  double cpu;
+  long nv, niv;
+  usage(&cpu, &nv, &niv);
+  size_t reserved = 0;
+  cudaMemPool_t pool;
+  if (device_pool(&pool) == cudaSuccess) {
+    uint64_t r = 0;
+    if (cudaMemPoolGetAttribute(pool, cudaMemPoolAttrReservedMemCurrent, &r) == cudaSuccess) reserved = r;
+  }
+  std::fprintf(stderr, "e2e_trace %s wall=%.2f cpu=%.2f vcsw=%ld ivcsw=%ld pool_mb=%.0f->%.0f |%s\n", name,
+               now_ms() - t0, cpu - cpu0, nv - nv0, niv - niv0, pool0 / 1048576.0, reserved / 1048576.0,
+               line.c_str());
+}
+
+void trace_mark(const char* what) {
+  if (g_trace) g_trace->mark(what);
 }
 }  // namespace e2e
 
@@ -87,6 +333,10 @@ extern "C" e2e_status e2e_memory_trim(void) {
   cudaMemPool_t pool;
   cudaError_t e = device_pool(&pool);
   if (e != cudaSuccess) return cuda_fail(e, "device_pool");
+  e = cudaDeviceSynchronize();
+  if (e != cudaSuccess) return cuda_fail(e, "cudaDeviceSynchronize");
+  const int dev = current_device();
+  if (dev >= 0) drop_cached(dev, 0);
   e = cudaDeviceSynchronize();
   if (e != cudaSuccess) return cuda_fail(e, "cudaDeviceSynchronize");
   e = cudaMemPoolTrimTo(pool, 0);
@@ -238,7 +488,7 @@ e2e_status upload(const void* src, size_t bytes, int where, void** dst, bool* ow
   if (bytes) {
     cudaError_t e = cudaMemcpyAsync(d, src, bytes, cudaMemcpyHostToDevice, st);
     if (e != cudaSuccess) {
-      cudaFreeAsync(d, st);
+      dfree(d, st);
       return cuda_fail(e, "cudaMemcpyAsync(fields)");
     }
   }
@@ -329,11 +579,11 @@ void free_model_buffers(e2e_model* m) {
     delete m->pack;
     m->pack = nullptr;
   }
-  if (m->row_ptr) cudaFreeAsync(m->row_ptr, 0);
-  if (m->col) cudaFreeAsync(m->col, 0);
-  if (m->cnt) cudaFreeAsync(m->cnt, 0);
-  if (m->R) cudaFreeAsync(m->R, 0);
-  if (m->sumR) cudaFreeAsync(m->sumR, 0);
+  dfree(m->row_ptr, 0);
+  dfree(m->col, 0);
+  dfree(m->cnt, 0);
+  dfree(m->R, 0);
+  dfree(m->sumR, 0);
   m->sumR = nullptr;
   m->row_ptr = nullptr;
   m->col = nullptr;
@@ -397,10 +647,12 @@ extern "C" e2e_status e2e_build_model(const e2e_problem* p, const e2e_fields* f,
   if (s != E2E_OK) return s;
   plan.keep_sums = o.keep_reward_parts != 0;
 
+  HostTrace trace("build_model");
   DeviceScratch scratch(st);
   FieldsOnDevice fd;
   s = fields_to_device(p, f, where, st, &fd, &scratch, /*defer=*/true);
   if (s != E2E_OK) return s;
+  trace.mark("fields");
 
   e2e_model* m = new (std::nothrow) e2e_model();
   if (!m) return fail(E2E_ERR_NOMEM, "host allocation");
@@ -411,6 +663,7 @@ extern "C" e2e_status e2e_build_model(const e2e_problem* p, const e2e_fields* f,
     return s;
   }
   CK(cudaStreamSynchronize(st));
+  trace.mark("done");
   *out = m;
   return E2E_OK;
 }
@@ -532,10 +785,12 @@ e2e_status run_build(const e2e_problem* p, const FieldsOnDevice& fd, const Build
   const int mm = p->neighb_gsize * p->neighb_gsize;
   cudaEvent_t ev[4];
   for (int k = 0; k < 4; ++k) CK(cudaEventCreate(&ev[k]));
+  trace_mark("events");
   struct EvFree {
     cudaEvent_t* e;
     ~EvFree() { for (int k = 0; k < 4; ++k) cudaEventDestroy(e[k]); }
   } evfree{ev};
+  trace_mark("setup");
   for (int attempt = 0; attempt < 3; ++attempt) {
     if (!stage_col) {
       CK(dalloc((void**)&stage_col, sizeof(int32_t) * (size_t)cap, st));
@@ -562,34 +817,42 @@ e2e_status run_build(const e2e_problem* p, const FieldsOnDevice& fd, const Build
     A.pool = pool;
     A.pool_units = pool_units;
     CK(cudaEventRecord(ev[0], st));
+    trace_mark("buffers");
     if (attempt == 0 && fd.n_deferred) {
-      // host fields: copy the first layers' steps, build them while the rest
-      // is copied on a second stream, then build the remaining layers
+      // host fields: copy the first layers' steps, then build them while the
+      // rest is copied on a second stream, then build the remaining layers
       const int la = std::max(1, std::min(p->nt - 1, (p->nt - 1) / 16));
       e2e_status cs = copy_field_steps(fd, 0, la + 1, st);
       if (cs != E2E_OK) return cs;
-      BuildArgs A0 = A;
-      CK(launch_build_tiles(A0, pl.count_bits, la, st));
-      m->build_launches++;
+      cudaStream_t cps = nullptr;
+      cudaEvent_t evs[2] = {nullptr, nullptr};
+      struct CopyFree {
+        cudaStream_t* s;
+        cudaEvent_t* e;
+        ~CopyFree() {
+          for (int k = 0; k < 2; ++k)
+            if (e[k]) cudaEventDestroy(e[k]);
+          if (*s) cudaStreamDestroy(*s);
+        }
+      } cpfree{&cps, evs};
       if (la < p->nt - 1) {
-        cudaStream_t cps = nullptr;
-        cudaEvent_t evs[2] = {nullptr, nullptr};
         CK(cudaStreamCreateWithFlags(&cps, cudaStreamNonBlocking));
-        struct CopyFree {
-          cudaStream_t s;
-          cudaEvent_t* e;
-          ~CopyFree() {
-            for (int k = 0; k < 2; ++k)
-              if (e[k]) cudaEventDestroy(e[k]);
-            if (s) cudaStreamDestroy(s);
-          }
-        } cpfree{cps, evs};
         for (int k = 0; k < 2; ++k) CK(cudaEventCreateWithFlags(&evs[k], cudaEventDisableTiming));
-        CK(cudaEventRecord(evs[0], st));  // the device buffers exist (stream-ordered allocations)
+        // after the buffers exist (stream-ordered allocations) and the first
+        // steps are in, before the first launch, so the copy runs beside it
+        CK(cudaEventRecord(evs[0], st));
         CK(cudaStreamWaitEvent(cps, evs[0], 0));
+        trace_mark("copy_stream");
         cs = copy_field_steps(fd, la + 1, p->nt, cps);
         if (cs != E2E_OK) return cs;
         CK(cudaEventRecord(evs[1], cps));
+        trace_mark("copies");
+      }
+      BuildArgs A0 = A;
+      CK(launch_build_tiles(A0, pl.count_bits, la, st));
+      m->build_launches++;
+      trace_mark("first_layers");
+      if (la < p->nt - 1) {
         CK(cudaStreamWaitEvent(st, evs[1], 0));
         BuildArgs A1 = A;
         A1.t0 = la;
@@ -600,12 +863,19 @@ e2e_status run_build(const e2e_problem* p, const FieldsOnDevice& fd, const Build
       CK(launch_build_tiles(A, pl.count_bits, p->nt - 1, st));
       m->build_launches++;
     }
+    trace_mark("launch");
     CK(cudaEventRecord(ev[1], st));
+    trace_mark("record");
+    // sleep through the builder; the counters' copy into host (stack) memory
+    // would otherwise spin until it finishes
+    CK(sleep_sync(st));
+    trace_mark("build");
     CK(cudaMemcpyAsync(hc, ctr, sizeof(hc), cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
+    trace_mark("counters");
     bool again = false;
     if (hc[CTR_FLAGS] & FLAG_POOL_EXHAUSTED) {
-      cudaFreeAsync(pool, st);
+      dfree(pool, st);
       pool = nullptr;
       pool_units = (int64_t)hc[CTR_POOL];
       if ((double)pool_units * mm * 4 > 32.0 * (1ull << 30))
@@ -613,8 +883,8 @@ e2e_status run_build(const e2e_problem* p, const FieldsOnDevice& fd, const Build
       again = true;
     }
     if ((int64_t)hc[CTR_STAGE] > cap) {
-      cudaFreeAsync(stage_col, st);
-      cudaFreeAsync(stage_cnt, st);
+      dfree(stage_col, st);
+      dfree(stage_cnt, st);
       stage_col = nullptr;
       stage_cnt = nullptr;
       cap = (int64_t)hc[CTR_STAGE];
@@ -647,6 +917,7 @@ e2e_status run_build(const e2e_problem* p, const FieldsOnDevice& fd, const Build
   CK(dalloc(&m->row_ptr, (size_t)pb * (size_t)(pl.n_rows + 1), st));
   CK(dalloc((void**)&m->col, sizeof(int32_t) * (size_t)(nnz + 16), st));
   CK(dalloc(&m->cnt, (size_t)cbytes * (size_t)(nnz + 16), st));
+  trace_mark("model_alloc");
   int64_t* canon = nullptr;
   int64_t* total = nullptr;
   CK(dalloc((void**)&canon, sizeof(int64_t) * (size_t)std::max<int64_t>(pl.n_tiles, 1), st));
@@ -657,7 +928,9 @@ e2e_status run_build(const e2e_problem* p, const FieldsOnDevice& fd, const Build
   int64_t* block_sums = nullptr;
   CK(dalloc((void**)&block_sums, sizeof(int64_t) * (size_t)(pl.n_tiles / 1024 + 2), st));
   scratch->add(block_sums);
+  trace_mark("scratch_alloc");
   CK(launch_scan_tiles(tile_len, pl.n_tiles, canon, total, block_sums, st));
+  trace_mark("scan_launch");
   AssembleArgs S;
   S.n_tiles = pl.n_tiles;
   S.tiles_per_layer = pl.etiles_per_layer;
@@ -677,7 +950,9 @@ e2e_status run_build(const e2e_problem* p, const FieldsOnDevice& fd, const Build
   S.cnt = m->cnt;
   CK(launch_assemble(S, pl.count_bits, m->index_bits, st));
   CK(cudaEventRecord(ev[3], st));
+  trace_mark("assemble_launch");
   CK(cudaEventSynchronize(ev[3]));
+  trace_mark("assemble");
   float ms = 0.f;
   CK(cudaEventElapsedTime(&ms, ev[0], ev[1]));
   m->build_kernel_ms = ms;
@@ -807,6 +1082,7 @@ e2e_status solve_on_device(const e2e_model* m, const e2e_vi_opts& o, float* dV, 
     e2e_status ps = ensure_pack(m, &pack_ms, st);
     if (ps != E2E_OK) return ps;
   }
+  trace_mark("pack");
   const ViPack& P = m->pack->v;
   DeviceScratch scratch(st);
   float* W = nullptr;
@@ -954,6 +1230,7 @@ extern "C" e2e_status e2e_spvi_solve(const e2e_model* m, const e2e_vi_opts* opts
   const int64_t ns = m->ns;
   float* dV = nullptr;
   int32_t* dpi = nullptr;
+  HostTrace trace("spvi_solve");
   DeviceScratch scratch(st);
   if (out_where == E2E_DEVICE && value_out) {
     dV = value_out;
@@ -969,10 +1246,12 @@ extern "C" e2e_status e2e_spvi_solve(const e2e_model* m, const e2e_vi_opts* opts
   }
   e2e_status s = solve_on_device(m, o, dV, dpi, stats, st);
   if (s != E2E_OK && s != E2E_ERR_NOT_CONVERGED && s != E2E_ERR_TIMEOUT) return s;
+  trace.mark("solve");
   if (out_where == E2E_HOST) {
     if (value_out) CK(cudaMemcpyAsync(value_out, dV, sizeof(float) * ns, cudaMemcpyDeviceToHost, st));
     if (policy_out) CK(cudaMemcpyAsync(policy_out, dpi, sizeof(int32_t) * ns, cudaMemcpyDeviceToHost, st));
   }
   CK(cudaStreamSynchronize(st));
+  trace.mark("outputs");
   return s;
 }

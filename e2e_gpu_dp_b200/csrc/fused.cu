@@ -103,12 +103,14 @@ extern "C" e2e_status e2e_build_solve(const e2e_problem* p, const e2e_fields* f,
       ++launches;
     }
     CK(cudaEventRecord(ev[1], st));
+    // sleep through the pass, then read its counters
+    CK(sleep_sync(st));
     CK(cudaMemcpyAsync(hc, ctr, sizeof(hc), cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
     if (!(hc[CTR_FLAGS] & FLAG_POOL_EXHAUSTED)) break;
     // rows that found no dense histogram were not backed up: again with the
     // pool size the pass asked for
-    cudaFreeAsync(pool, st);
+    dfree(pool, st);
     pool = nullptr;
     pool_units = (int64_t)hc[CTR_POOL];
     if ((double)pool_units * mm * 4 > 32.0 * (1ull << 30))

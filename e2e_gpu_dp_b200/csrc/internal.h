@@ -36,9 +36,36 @@ struct e2e_model {
 namespace e2e {
 
 e2e_status fail(e2e_status st, const std::string& msg);
-// device allocation from the library's stream-ordered pool (free with cudaFreeAsync)
+// device allocation from the library's stream-ordered pool, large blocks through
+// the library's block cache; release with dfree on the stream that last uses it
 cudaError_t dalloc(void** p, size_t bytes, cudaStream_t st);
+void dfree(void* p, cudaStream_t st);
 e2e_status cuda_fail(cudaError_t e, const char* what);
+// wait for the work queued on st with the calling thread asleep (a blocking-sync
+// event) rather than spinning: for waits on long builder launches
+cudaError_t sleep_sync(cudaStream_t st);
+
+// Host-side phase trace, for finding where a call's wall time goes: with
+// E2E_TRACE=1 in the environment, each traced call prints one line to stderr
+// with the milliseconds between its marks, its wall and CPU time, its voluntary
+// and involuntary context switches, and the bytes the device pool holds.  Off,
+// a mark is one branch on a thread-local pointer.
+struct HostTrace {
+  explicit HostTrace(const char* name);
+  ~HostTrace();
+  HostTrace(const HostTrace&) = delete;
+  HostTrace& operator=(const HostTrace&) = delete;
+  void mark(const char* what);
+  bool on = false;
+  const char* name;
+  double t0 = 0, last = 0, cpu0 = 0;
+  size_t pool0 = 0;
+  long nv0 = 0, niv0 = 0;
+  HostTrace* prev = nullptr;
+  std::string line;
+};
+// mark on the trace active on this thread, if any
+void trace_mark(const char* what);
 
 // Stream-ordered temporaries released when the owner goes out of scope.
 struct DeviceScratch {
@@ -49,7 +76,7 @@ struct DeviceScratch {
     if (p) ptrs.push_back(p);
   }
   ~DeviceScratch() {
-    for (void* p : ptrs) cudaFreeAsync(p, st);
+    for (void* p : ptrs) dfree(p, st);
   }
   DeviceScratch(const DeviceScratch&) = delete;
   DeviceScratch& operator=(const DeviceScratch&) = delete;

@@ -195,7 +195,7 @@ struct Server {
   void free_model(ModelEntry* me) {
     used -= me->bytes;
     e2e_model_free(me->m);
-    for (void* p : me->owned) cudaFreeAsync(p, st);
+    for (void* p : me->owned) dfree(p, st);
     delete me;
   }
 
@@ -279,9 +279,9 @@ struct Server {
   }
 
   void release(Req* q) {
-    if (q->V) cudaFreeAsync(q->V, st);
-    if (q->pi) cudaFreeAsync(q->pi, st);
-    if (q->Rwin) cudaFreeAsync(q->Rwin, st);
+    dfree(q->V, st);
+    dfree(q->pi, st);
+    dfree(q->Rwin, st);
     q->V = nullptr;
     q->pi = nullptr;
     q->Rwin = nullptr;

@@ -900,7 +900,7 @@ int occupancy(const void* kern) {
 void free_pack(PackStore* p) {
   if (!p) return;
   for (void*& b : p->bufs) {
-    if (b) cudaFreeAsync(b, 0);
+    dfree(b, 0);
     b = nullptr;
   }
 }
@@ -937,9 +937,9 @@ cudaError_t build_pack(const ViModel& M, int64_t nc, int g, int del, PackStore* 
   int64_t* block_sums = nullptr;
   unsigned int* flags = nullptr;
   auto cleanup = [&]() {
-    if (slot_len) cudaFreeAsync(slot_len, st);
-    if (block_sums) cudaFreeAsync(block_sums, st);
-    if (flags) cudaFreeAsync(flags, st);
+    dfree(slot_len, st);
+    dfree(block_sums, st);
+    dfree(flags, st);
   };
   const int64_t nb = (P.nchunks + 1023) / 1024 + 1;
   if ((e = dalloc(&out->bufs[0], sizeof(int64_t) * (P.nchunks + 1), st)) != cudaSuccess) return e;
@@ -995,8 +995,8 @@ cudaError_t build_pack(const ViModel& M, int64_t nc, int g, int del, PackStore* 
     if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return cleanup(), e;
     if (!(hf & 1u) || P.ent_mode == ENT_I32) break;
     // a column outside the window: repack with int32 columns
-    cudaFreeAsync(out->bufs[2], st);
-    if (out->bufs[3]) cudaFreeAsync(out->bufs[3], st);
+    dfree(out->bufs[2], st);
+    dfree(out->bufs[3], st);
     out->bufs[2] = out->bufs[3] = nullptr;
     P.ent_mode = ENT_I32;
   }
