@@ -554,6 +554,17 @@ __global__ void __launch_bounds__(1024) k_build_tiles(BuildArgs A) {
       if (plain_warp) {
         // counts only: the rewards are folded from the counters at the end, a
         // sample that leaves the window counts in the miss bin
+        // The window origin is folded into the rounding constant: the bits of
+        // RD(w + 1.5*2^23 - wj0) are 0x4B400000 + lj (exact while |w - wj0| <
+        // 2^22, the floats there being the integers), so one three-input logic
+        // op tests both coordinates, and the counter's 32-bit shared address
+        // is base + (8*by + bx) << sh with the offset 9*0x4B400000 folded into
+        // the base, modulo 2^32 (200x200x120 builder 413 -> 409 ms).
+        const uint32_t M = 0x4B400000u;
+        const float2 magic = make_float2(12582912.0f - (float)wj0, 12582912.0f - (float)wi0);
+        const uint32_t sh = (uint32_t)log2S + 1u;  // bytes per bin row, log2
+        const uint32_t base_adj = (uint32_t)__cvta_generic_to_shared(wcol) - ((9u * M) << sh);
+        const uint32_t miss_idx = 9u * M + (uint32_t)kMissBin;
 #pragma unroll 16
         for (int q = 0; q < clen; ++q) {
           const float2 vv = myvel[q];
@@ -561,16 +572,20 @@ __global__ void __launch_bounds__(1024) k_build_tiles(BuildArgs A) {
           // (xnew - xs0, -(ynew - ysn)) without the domain clamps: a plain
           // row's window holds no edge cell, so a sample the clamps would move
           // lands outside the window either way (unclamped its index is below 0
-          // or above g-1; a NaN or a value beyond 2^22 gives bits far from the
-          // bias) and is taken again by the rescan below
+          // or above g-1; a NaN or a value beyond 2^22 gives bits far from
+          // 0x4B400000) and is taken again by the rescan below
           const float2 d = __ffma2_rn(xy, sgn, org);
-          int lj, li;
-          round_half_up_index2(d, kx, ky, lj, li);
-          const bool inw = (unsigned)(li | lj) < (unsigned)kWin;
-          const int b = inw ? (li << 3) + lj : kMissBin;
-          uint16_t* wp = wcol + (b << log2S);
-          *wp = (uint16_t)(*wp + 1);
+          const float2 w = __fadd2_rd(d, make_float2(0.5f, 0.5f));  // round_half_up_index
+          const float2 t = __fadd2_rd(w, magic);
+          const uint32_t bx = __float_as_uint(t.x), by = __float_as_uint(t.y);
+          const bool inw = ((bx ^ M) | (by ^ M)) < (uint32_t)kWin;
+          const uint32_t addr = base_adj + ((inw ? (by << 3) + bx : miss_idx) << sh);
+          unsigned short v;
+          asm volatile("ld.shared.u16 %0, [%1];" : "=h"(v) : "r"(addr));
+          v = (unsigned short)(v + 1);
+          asm volatile("st.shared.u16 [%0], %1;" ::"r"(addr), "h"(v));
         }
+        asm volatile("" ::: "memory");  // the counters are read below
         uint16_t* mp = wcol + (kMissBin << log2S);
         n_out = *mp;
         if (n_out) *mp = 0;
