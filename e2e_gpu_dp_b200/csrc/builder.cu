@@ -583,16 +583,23 @@ __global__ void __launch_bounds__(1024) k_build_tiles(BuildArgs A) {
           v = (unsigned short)(v + 1);
           asm volatile("st.shared.u16 [%0], %1;" ::"r"(addr), "h"(v));
         };
-        // two realisations a 16-byte load (the velocity rows have an even
-        // stride): 200x200x120 builder 409 -> 393 ms
-        int q = 0;
+        if constexpr (FUSED) {
+          // one realisation a load: the fused instance measured 444 ms with
+          // the pairs below and 419 ms without them (200x200x120)
+#pragma unroll 16
+          for (int q = 0; q < clen; ++q) count_sample(myvel[q]);
+        } else {
+          // two realisations a 16-byte load (the velocity rows have an even
+          // stride): 200x200x120 builder 409 -> 393 ms
+          int q = 0;
 #pragma unroll 8
-        for (; q + 1 < clen; q += 2) {
-          const float4 v2 = *reinterpret_cast<const float4*>(myvel + q);
-          count_sample(make_float2(v2.x, v2.y));
-          count_sample(make_float2(v2.z, v2.w));
+          for (; q + 1 < clen; q += 2) {
+            const float4 v2 = *reinterpret_cast<const float4*>(myvel + q);
+            count_sample(make_float2(v2.x, v2.y));
+            count_sample(make_float2(v2.z, v2.w));
+          }
+          if (q < clen) count_sample(myvel[q]);
         }
-        if (q < clen) count_sample(myvel[q]);
         asm volatile("" ::: "memory");  // the counters are read below
         uint16_t* mp = wcol + (kMissBin << log2S);
         n_out = *mp;
