@@ -326,6 +326,35 @@ __global__ void k_env_cloud(CloudArgs a) {
 // row-major buffer is the column-major ncols x nws matrix X^T, which gesvdj
 // takes directly when ncols >= nws (X^T = U S V^T: X's left vectors are V);
 // otherwise X is transposed into column-major nws x ncols first.
+// cuSOLVER and cuBLAS handles, one pair per host thread and device, kept for
+// the thread's lifetime (never destroyed: a thread-exit destructor could run
+// after the CUDA context is gone).  Creating them on every call allocated
+// their device work space through the driver each time, which on a busy
+// machine added tens of milliseconds to a 35 ms generation.
+e2e_status solver_handles(cusolverDnHandle_t* sol, cublasHandle_t* blas) {
+  struct Pair {
+    cusolverDnHandle_t sol;
+    cublasHandle_t blas;
+  };
+  thread_local Pair h[64] = {};
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return cuda_fail(e, "cudaGetDevice");
+  if (dev < 0 || dev >= 64) return fail(E2E_ERR_UNSUPPORTED, "device index above 63");
+  Pair& x = h[dev];
+  if (!x.sol && cusolverDnCreate(&x.sol) != CUSOLVER_STATUS_SUCCESS) {
+    x.sol = nullptr;
+    return fail(E2E_ERR_CUDA, "cusolverDnCreate");
+  }
+  if (!x.blas && cublasCreate(&x.blas) != CUBLAS_STATUS_SUCCESS) {
+    x.blas = nullptr;
+    return fail(E2E_ERR_CUDA, "cublasCreate");
+  }
+  *sol = x.sol;
+  *blas = x.blas;
+  return E2E_OK;
+}
+
 struct SvdWork {
   cusolverDnHandle_t sol = nullptr;
   cublasHandle_t blas = nullptr;
@@ -562,13 +591,13 @@ extern "C" e2e_status e2e_env_generate(const e2e_env_params* p, const int32_t* i
     SvdWork* w;
     ~SvdFree() {
       if (w->params) cusolverDnDestroyGesvdjInfo(w->params);
-      if (w->sol) cusolverDnDestroy(w->sol);
-      if (w->blas) cublasDestroy(w->blas);
     }
   } svdfree{&w};
-  if (cusolverDnCreate(&w.sol) != CUSOLVER_STATUS_SUCCESS) return fail(E2E_ERR_CUDA, "cusolverDnCreate");
+  {
+    e2e_status hs = solver_handles(&w.sol, &w.blas);
+    if (hs != E2E_OK) return hs;
+  }
   CKS(cusolverDnSetStream(w.sol, st));
-  if (cublasCreate(&w.blas) != CUBLAS_STATUS_SUCCESS) return fail(E2E_ERR_CUDA, "cublasCreate");
   CKB(cublasSetStream(w.blas, st));
   CKB(cublasSetPointerMode(w.blas, CUBLAS_POINTER_MODE_HOST));
   CKS(cusolverDnCreateGesvdjInfo(&w.params));
