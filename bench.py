@@ -220,15 +220,52 @@ def algorithmic_build_bytes(prob, nnz: int, count_bytes: int) -> int:
     return int(reads + writes)
 
 
-def cpu_baseline(prob, fields, threads: int, target_s: float = 15.0):
-    """The oracle (C restatement) on a bounded sample of rows, extrapolated."""
+def workload_config(prob, ws: int = 1) -> dict:
+    """The bench line's ``config``: the same dict in both arms."""
+    return {
+        "workload": "single large solve: 200x200 grid, nt=120, 16 headings, F=1, nrzns=5000, "
+                    "10 modes sigma_k=0.3/2^(k/2), gyre A=1, 3% obstacles, seed 1234",
+        "states": prob.ns, "rows": (prob.nt - 1) * prob.ncells * prob.num_actions,
+        "samples": (prob.nt - 1) * prob.ncells * prob.num_actions * prob.nrzns,
+        "parallelism": f"replicas x{ws}", "l2": "inputs (fields 0.45 GB, model 2.2 GB) exceed L2",
+    }
+
+
+def vi_bytes_per_iteration(ns: int, na: int, nnz: int, count_bytes: int) -> int:
+    """Algorithmic bytes of one VI sweep over the CSR with a per-state row
+    pointer: nnz*(b_cnt + 4) + (Ns + 1)*4 + Na*Ns*4 + 3*Ns*4 (entries, row
+    pointer, R, V gathered once, V' and the policy written)."""
+    return int(nnz * (count_bytes + 4) + (ns + 1) * 4 + na * ns * 4 + 3 * ns * 4)
+
+
+def k1_issue_roofline(samples: int, k1_s: float, sm_mhz: float, n_sm: int):
+    """K1 is bound by instruction issue: warp instructions it issues (per-sample
+    count from the ncu capture in profiles/, times the samples) over the SMs'
+    issue capacity (4 schedulers x 1 warp instruction per cycle per SM at the
+    SM clock measured during the timed steps)."""
+    path = os.path.join(ROOT, "profiles", "traffic.json")
+    try:
+        per_sample = float(json.load(open(path))[f"k_build_tiles/{WORKLOAD}/warp_inst_per_sample"])
+    except Exception:
+        return None
+    inst = per_sample * samples
+    achieved = inst / k1_s
+    peak = n_sm * 4 * sm_mhz * 1e6
+    return {"warp_inst_per_sample": per_sample, "warp_inst": inst, "achieved": achieved, "peak": peak}
+
+
+def cpu_baseline(prob, fields, threads: int, target_s: float = 15.0, trig=None):
+    """The oracle (C restatement) on a bounded sample of rows, extrapolated.
+    Returns the baseline and the sampled row blocks [(r0, rows)] (built with
+    ``trig``, the device's cos/sin of the headings, so they can be compared
+    with the device's rows bit for bit)."""
     from oracle import pyoracle as O
 
     n_rows = (prob.nt - 1) * prob.ncells * prob.num_actions
     # calibrate on a small block, then run a block sized for ~target_s
     probe = 2048
     t0 = time.perf_counter()
-    O.build_rows(prob, fields, r0=n_rows // 2, r1=n_rows // 2 + probe, nthreads=threads)
+    O.build_rows(prob, fields, trig=trig, r0=n_rows // 2, r1=n_rows // 2 + probe, nthreads=threads)
     dt = time.perf_counter() - t0
     rows = int(min(n_rows, max(probe, probe * target_s / max(dt, 1e-6))))
     chunks = 8
@@ -236,11 +273,13 @@ def cpu_baseline(prob, fields, threads: int, target_s: float = 15.0):
     t0 = time.perf_counter()
     done = 0
     nnz = 0
+    blocks = []
     for c in range(chunks):
         r0 = int((c + 0.5) * n_rows / chunks) - per // 2
-        out = O.build_rows(prob, fields, r0=r0, r1=r0 + per, nthreads=threads)
+        out = O.build_rows(prob, fields, trig=trig, r0=r0, r1=r0 + per, nthreads=threads)
         done += per
         nnz += len(out["col"])
+        blocks.append((r0, out))
     el = time.perf_counter() - t0
     est_build = el * n_rows / done
     # FP64 backward sweep: time on the sampled rows and scale by nnz
@@ -256,7 +295,32 @@ def cpu_baseline(prob, fields, threads: int, target_s: float = 15.0):
         "sample": f"oracle build of {done} of {n_rows} rows ({chunks} blocks spread over the layers) "
                   f"in {el:.1f}s on {threads} threads, extrapolated linearly; VI one FP64 sweep "
                   f"estimated from the sampled rows",
-    }
+    }, blocks
+
+
+def parity_sample(h, blocks, integer_rewards: bool = True) -> dict:
+    """Device rows against the oracle's rows of the same blocks: row lengths,
+    next states and counts bit for bit, rewards bit for bit (integer rewards)."""
+    rows = entries = bad_rows = 0
+    for r0, o in blocks:
+        n = len(o["row_ptr"]) - 1
+        rp = h["row_ptr"][r0:r0 + n + 1].astype(np.int64)
+        e0, e1 = int(rp[0]), int(rp[-1])
+        col, cnt = h["col"][e0:e1].astype(np.int64), h["cnt"][e0:e1].astype(np.int64)
+        orp = o["row_ptr"].astype(np.int64)
+        same_len = (rp - rp[0]) == (orp - orp[0])
+        if np.all(same_len):
+            diff = (col != o["col"].astype(np.int64)) | (cnt != o["cnt"].astype(np.int64))
+            bad = np.zeros(n, bool)
+            if diff.any():
+                bad[np.searchsorted(orp[1:] - orp[0], np.nonzero(diff)[0], side="right")] = True
+        else:
+            bad = ~(same_len[1:] & same_len[:-1])
+        r_bad = h["R"][r0:r0 + n] != o["R"] if integer_rewards else np.zeros(n, bool)
+        bad_rows += int(np.sum(bad | r_bad))
+        rows += n
+        entries += len(o["col"])
+    return {"rows": rows, "entries": entries, "mismatched_rows": bad_rows}
 
 
 def run_ours(args, ws, rank, local):
@@ -273,20 +337,25 @@ def run_ours(args, ws, rank, local):
     V = torch.empty(prob.ns, dtype=torch.float32, device="cuda")
     pi = torch.empty(prob.ns, dtype=torch.int32, device="cuda")
 
-    def step(record=None):
-        r0 = resource.getrusage(resource.RUSAGE_SELF)
+    def step(ev0=None, ev1=None):
+        """Build + layered solve between the events ev0/ev1 (both calls return
+        after their stream work is done); the model's info and its free come
+        after ev1, outside the timed region.  Returns (info, solve stats, host
+        ms of the two calls) when timed."""
+        if ev0 is not None:
+            ev0.record(stream)
         t0 = time.perf_counter()
         m = api.build_model(prob, dev, stream=stream)
         t1 = time.perf_counter()
         _, _, st = m.solve(method="layered", value=V, policy=pi, stream=stream)
         t2 = time.perf_counter()
-        if record is not None:
-            r1 = resource.getrusage(resource.RUSAGE_SELF)
-            host = {"cpu_ms": round((r1.ru_utime + r1.ru_stime - r0.ru_utime - r0.ru_stime) * 1e3, 1),
-                    "involuntary_switches": r1.ru_nivcsw - r0.ru_nivcsw,
-                    "page_faults": r1.ru_minflt - r0.ru_minflt + r1.ru_majflt - r0.ru_majflt}
-            record.append((m.info(), st, (round((t1 - t0) * 1e3, 1), round((t2 - t1) * 1e3, 1)), host))
+        if ev1 is None:
+            m.free()
+            return None
+        ev1.record(stream)
+        inf = m.info()
         m.free()
+        return inf, st, (round((t1 - t0) * 1e3, 1), round((t2 - t1) * 1e3, 1))
 
     recs = []
     starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
@@ -307,10 +376,14 @@ def run_ours(args, ws, rank, local):
         # each step between its own events: the clock sample taken between two
         # steps (host only, GPU idle) is not part of either
         for k in range(args.steps):
-            starts[k].record(stream)
-            step(recs)
-            ends[k].record(stream)
+            r0 = resource.getrusage(resource.RUSAGE_SELF)
+            inf, st, host_ms = step(starts[k], ends[k])
             torch.cuda.synchronize()
+            r1 = resource.getrusage(resource.RUSAGE_SELF)
+            usage = {"cpu_ms": round((r1.ru_utime + r1.ru_stime - r0.ru_utime - r0.ru_stime) * 1e3, 1),
+                     "involuntary_switches": r1.ru_nivcsw - r0.ru_nivcsw,
+                     "page_faults": r1.ru_minflt - r0.ru_minflt + r1.ru_majflt - r0.ru_majflt}
+            recs.append((inf, st, host_ms, usage))
             clk.tick()
         torch.cuda.synchronize()
         gc.enable()
@@ -374,10 +447,41 @@ def run_ours(args, ws, rank, local):
     m = api.build_model(prob, dev, stream=stream)
     _, _, jst = m.solve(method="jacobi", threshold=0.1, value=V, policy=pi, stream=stream)
     _, _, lst = m.solve(method="layered", fp64_check=True, value=V, policy=pi, stream=stream)
+    minf = m.info()
+    # parity: the device's rows against the oracle's rows of the CPU baseline's
+    # sample (same seeded inputs, the device's heading cos/sin), and the values
+    # against an FP64 backward induction on the host over the device's model
+    check = None
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        tab = api.action_table(prob)
+        baseline, blocks = cpu_baseline(prob, fields, threads=os.cpu_count() or 1,
+                                        trig=(tab["cos"], tab["sin"]))
+        h = m.to_host()
+        check = {"parity_sample": parity_sample(h, blocks)}
+        del blocks
+        from oracle import pyoracle as O
+        Vh = V.cpu().numpy().astype(np.float64)
+        pih = pi.cpu().numpy()
+        tf = time.perf_counter()
+        V64, _, gap = O.vi_f64_layers(prob.ncells, prob.nt, prob.num_actions, h["row_ptr"], h["col"],
+                                      h["cnt"], prob.nrzns, h["R"], policy=pih,
+                                      nthreads=os.cpu_count() or 1)
+        scale = float(np.max(np.abs(V64)))
+        band = 2e-5 * max(1.0, scale)
+        check["fp64_oracle"] = {
+            "kind": "oracle/e2e_oracle.c FP64 backward induction on the host over the device's model",
+            "seconds": round(time.perf_counter() - tf, 2),
+            "max_rel_err": float(np.max(np.abs(Vh - V64)) / scale),
+            "policy_mismatches_outside_ties": int(np.sum(gap > band)),
+            "policy_differs_within_ties": int(np.sum((gap > 0) & (gap <= band))),
+            "tie_band": band}
+        del h, V64, gap
     m.free()
     hbm, peak_kind = _peaks()
+    cb = 2 if minf["count_type"] == 0 else 4
+    vi_bytes = vi_bytes_per_iteration(prob.ns, prob.num_actions, minf["nnz"], cb)
     vi_gbs = jst["stream_bytes_per_sweep"] * jst["iterations"] / jst["seconds"] / 1e9
-    vi_csr_gbs = jst["bytes_per_sweep"] * jst["iterations"] / jst["seconds"] / 1e9
+    vi_alg_gbs = vi_bytes * jst["iterations"] / jst["seconds"] / 1e9
 
     # policy rollout evaluation of the solved c2 policy from the reference
     # script's start cell (int(0.5 g), int(0.95 g)), every realisation, against
@@ -424,19 +528,34 @@ def run_ours(args, ws, rank, local):
              "identical_to_build_then_solve": bool(torch.equal(Vf, V) and torch.equal(pif, pi)),
              "speedup_vs_step": round(ms / statistics.median(fused_ms), 3)}
 
-    cb = 2 if info["count_type"] == 0 else 4
     k1_bytes = algorithmic_build_bytes(prob, info["nnz"], cb)
     k1_gbs = k1_bytes / (k1_ms * 1e-3) / 1e9
     traffic = None
     tpath = os.path.join(ROOT, "profiles", "traffic.json")
     if os.path.exists(tpath):
         try:
-            traffic = json.load(open(tpath)).get(f"k_build_tiles/{WORKLOAD}")
+            traffic = json.load(open(tpath)).get(f"k_build_tiles/{WORKLOAD}/dram_bytes")
         except Exception:
             traffic = None
     samples = (prob.nt - 1) * prob.ncells * prob.num_actions * prob.nrzns
 
     value_s = whole_job_seconds_per_solve(ms, ws)
+    n_sm = torch.cuda.get_device_properties(local).multi_processor_count
+    sm_mhz = clocks["sm_mhz"] if clocks else 1965.0
+    issue = k1_issue_roofline(samples, k1_ms * 1e-3, sm_mhz, n_sm)
+    hbm_part = {"achieved": round(k1_gbs, 2), "peak": hbm, "unit": "GB/s", "frac": round(k1_gbs / hbm, 5),
+                "traffic": traffic, "peak_source": f"{peak_kind} hbm_gbs", "algorithmic_bytes": k1_bytes}
+    if issue is not None:
+        roof = {"kernel": "k_build_tiles", "bound": "issue", "achieved": round(issue["achieved"], 1),
+                "peak": round(issue["peak"], 1), "unit": "warp-inst/s",
+                "frac": round(issue["achieved"] / issue["peak"], 4), "traffic": traffic,
+                "warp_inst_per_sample": issue["warp_inst_per_sample"], "sm_mhz": sm_mhz, "sms": n_sm,
+                "note": "issue-bound Monte-Carlo kernel: warp instructions (per-sample count of the ncu "
+                        "capture in profiles/k_build_tiles_c2nt30.md x samples) / K1 time, against 4 warp "
+                        "instructions per cycle per SM at the measured SM clock; its HBM figure below",
+                "hbm": hbm_part}
+    else:
+        roof = {"kernel": "k_build_tiles", "bound": "hbm", **hbm_part}
     line = {
         "metric": "build+VI sec",
         "value": round(value_s, 6),
@@ -450,13 +569,9 @@ def run_ours(args, ws, rank, local):
         "vs_baseline": None,
         "dtype": "fp32 values, u16 counts, fp64 residual",
         "data": "synthetic (seeded double gyre + Fourier modes, reference layout)",
-        "config": {
-            "workload": "single large solve: 200x200 grid, nt=120, 16 headings, F=1, nrzns=5000, "
-                        "10 modes sigma_k=0.3/2^(k/2), gyre A=1, 3% obstacles",
-            "states": prob.ns, "rows": info["n_rows"], "nnz": info["nnz"], "samples": samples,
-            "solve": "layered backward sweep + FP64-residual verification sweep",
-            "parallelism": f"replicas x{ws}", "l2": "inputs (fields 0.45 GB, model 2.2 GB) exceed L2",
-        },
+        "config": workload_config(prob, ws),
+        "nnz": info["nnz"],
+        "solve": "layered backward sweep + FP64-residual verification sweep",
         "e2e": {"value": round(e2e_ms / 1e3 / ws, 6), "unit": "s", "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": d2h, "step_wall_ms": e2e_steps,
                 "step_build_solve_wall_ms": e2e_split},
@@ -470,20 +585,17 @@ def run_ours(args, ws, rank, local):
         "phases_ms": {"build_kernel": round(k1_ms, 3), "assemble": round(asm_ms, 3),
                       "pack": round(pack_ms, 3), "solve": round(solve_ms, 3),
                       "layered_pass": round(pass_ms, 3)},
-        "roofline": {"kernel": "k_build_tiles", "bound": "hbm", "achieved": round(k1_gbs, 2),
-                     "peak": hbm, "unit": "GB/s", "frac": round(k1_gbs / hbm, 5),
-                     "traffic": traffic, "peak_source": f"{peak_kind} hbm_gbs",
-                     "algorithmic_bytes": k1_bytes,
-                     "note": "issue-bound Monte-Carlo kernel; samples/s is its throughput"},
+        "roofline": roof,
         "build_samples_per_s": round(samples / (k1_ms * 1e-3), 1),
         "vi": {"kernel": "k_vi_chunks (Jacobi, reference schedule)", "iterations": jst["iterations"],
-               "algorithmic_bytes_per_sweep": jst["bytes_per_sweep"],
+               "algorithmic_bytes_per_sweep": vi_bytes,
                "moved_bytes_per_sweep": jst["stream_bytes_per_sweep"], "seconds": round(jst["seconds"], 6),
-               "achieved_gbs": round(vi_csr_gbs, 1), "frac": round(vi_csr_gbs / hbm, 4),
+               "achieved_gbs": round(vi_alg_gbs, 1), "peak": hbm, "frac": round(vi_alg_gbs / hbm, 4),
                "moved_gbs": round(vi_gbs, 1), "moved_frac": round(vi_gbs / hbm, 4),
-               "note": "algorithmic bytes: the CSR sweep (row_ptr, col, count, R, V read, V and policy "
-                       "written); moved: the sliced copy actually streamed (no row_ptr, packed entries, "
-                       "padding)",
+               "note": "algorithmic bytes per sweep: nnz*(b_cnt+4) + (Ns+1)*4 + Na*Ns*4 + 3*Ns*4 "
+                       "(entries, per-state row pointer, R, V gathered once, V' and the policy written); "
+                       "moved: the sliced copy actually streamed (packed entries, R, padding)",
+               "per_row_pointer_bytes_per_sweep": jst["bytes_per_sweep"],
                "layered_seconds": round(lst["seconds"], 6),
                "layered_pass_seconds": round(lst["sweep_seconds"], 6),
                "fp64_max_rel_err": lst["fp64_max_rel_err"]},
@@ -491,8 +603,9 @@ def run_ours(args, ws, rank, local):
         "fused_build_solve": fused,
         "clocks": clocks,
     }
-    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
-        line["cpu_baseline"] = cpu_baseline(prob, fields, threads=os.cpu_count() or 1)
+    if check is not None:
+        line["cpu_baseline"] = baseline
+        line.update(check)
     return line
 
 
@@ -756,11 +869,15 @@ def run_envgen() -> dict:
     return res
 
 
-def run_precision() -> dict:
+def run_precision(sample_rows: int = 80000) -> dict:
     """Precision form: 300x300 grid, nt=150 (13.5 M states), 16 headings,
     nrzns 2000, 8 modes; uint16 counts with int32 next states, FP32 values, the
     FP64 Bellman residual of the verification sweep, and an FP64 backward solve
-    on the GPU as the check (max |V32 - V64| / max |V64|)."""
+    on the GPU as the library's own check (max |V32 - V64| / max |V64|).  Then
+    two checks that do not use the library: ``sample_rows`` rows built by the
+    oracle against the device's, and an FP64 backward induction on the host
+    (the oracle) over the device's model: value error and policy mismatches
+    outside the FP64 tie band."""
     import torch
 
     from e2e_gpu_dp_b200 import api
@@ -780,7 +897,46 @@ def run_precision() -> dict:
     wall = time.perf_counter() - t0
     _, _, chk = m.solve(method="layered", fp64_check=True, value=V, policy=pi, stream=stream)
     inf = m.info()
+    # independent checks on the host: the oracle's rows of 8 blocks spread over
+    # the layers against the device's, bit for bit; an FP64 backward induction
+    # (the oracle, on the host) over the device's model copied down: value error
+    # and the policy's FP64 margin (actions more than the tie band below the
+    # best are mismatches)
+    from e2e_gpu_dp_b200.problem import make_fields
+    from oracle import pyoracle as O
+
+    threads = os.cpu_count() or 1
+    h = m.to_host()
     m.free()
+    fields = make_fields(prob, spec)
+    tab = api.action_table(prob)
+    n_rows = (prob.nt - 1) * prob.ncells * prob.num_actions
+    per = sample_rows // 8
+    blocks = []
+    ts = time.perf_counter()
+    for c in range(8):
+        r0 = int((c + 0.5) * n_rows / 8) - per // 2
+        blocks.append((r0, O.build_rows(prob, fields, trig=(tab["cos"], tab["sin"]), r0=r0, r1=r0 + per,
+                                        nthreads=threads)))
+    sample_s = time.perf_counter() - ts
+    par = parity_sample(h, blocks)
+    del blocks, fields
+    tf = time.perf_counter()
+    V64, _, gap = O.vi_f64_layers(prob.ncells, prob.nt, prob.num_actions, h["row_ptr"], h["col"],
+                                  h["cnt"], prob.nrzns, h["R"], policy=pi.cpu().numpy(),
+                                  nthreads=threads)
+    f64_s = time.perf_counter() - tf
+    scale = float(np.max(np.abs(V64)))
+    band = 2e-5 * max(1.0, scale)
+    Vh = V.cpu().numpy().astype(np.float64)
+    host_check = {"kind": "oracle/e2e_oracle.c FP64 backward induction on the host over the device's model",
+                  "threads": threads, "seconds": round(f64_s, 2),
+                  "max_abs_err": float(np.max(np.abs(Vh - V64))),
+                  "max_rel_err": float(np.max(np.abs(Vh - V64)) / scale),
+                  "policy_mismatches_outside_ties": int(np.sum(gap > band)),
+                  "policy_differs_within_ties": int(np.sum((gap > 0) & (gap <= band))),
+                  "tie_band": band}
+    del h, V64, gap
     return {"workload": "300x300 grid, nt=150, 16 headings, nrzns 2000, 8 modes, uint16 counts",
             "states": prob.ns, "rows": inf["n_rows"], "nnz": inf["nnz"],
             "count_type": "u16" if inf["count_type"] == 0 else inf["count_type"],
@@ -788,7 +944,9 @@ def run_precision() -> dict:
             "pack_ms": round(st["pack_ms"], 2), "solve_ms": round(st["seconds"] * 1e3, 3),
             "layered_pass_ms": round(st["sweep_seconds"] * 1e3, 3), "build_solve_wall_s": round(wall, 3),
             "fp64_residual": chk["residual"], "fp64_max_abs_err": chk["fp64_max_abs_err"],
-            "fp64_max_rel_err": chk["fp64_max_rel_err"]}
+            "fp64_max_rel_err": chk["fp64_max_rel_err"],
+            "fp64_oracle": host_check,
+            "parity_sample": {**par, "oracle_s": round(sample_s, 2), "threads": threads}}
 
 
 def run_reference(args, ws, rank, local):
@@ -832,8 +990,8 @@ def run_reference(args, ws, rank, local):
         "vs_baseline": None,
         "dtype": "fp32",
         "data": "synthetic (same seeded inputs as the ours arm)",
-        "config": {"workload": "single large solve: 200x200 grid, nt=120, 16 headings, F=1, "
-                               "nrzns=5000, 10 modes", "pipeline": "build_model -> convert -> spvi_2"},
+        "config": workload_config(prob, 1),
+        "pipeline": "build_model -> convert -> spvi_2",
         "phases_s": {"build_loop": statistics.mean(r["build_loop_s"] for r in runs),
                      "build_process": statistics.mean(r["wall_build_s"] for r in runs),
                      "convert": statistics.mean(r["wall_convert_s"] for r in runs),

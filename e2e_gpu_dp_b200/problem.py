@@ -360,4 +360,28 @@ def config(name: str, seed: int = 1234) -> Tuple[Problem, FieldSpec]:
         return (Problem(gsize=24, nt=6, nrzns=400, nmodes=4, num_ac_angles=8, F=1.0,
                         i_term=20, j_term=20, neighb_gsize=21, prob_name="t_wide"),
                 FieldSpec(A=0.5, sigma0=1.2, sigma_base=1.5, obstacle_frac=0.03, seed=seed))
+    # The single-large-solve and precision workloads in small: their heading
+    # count, mode count, realisation count, gyre and noise, on a small grid.
+    if name == "t_m10":        # 200x200x120's per-row shape: 16 headings, 10 modes, 5000 realisations
+        return (Problem(gsize=22, nt=4, nrzns=5000, nmodes=10, num_ac_angles=16, F=1.0,
+                        i_term=18, j_term=10, neighb_gsize=21, prob_name="t_m10"),
+                FieldSpec(A=1.0, sigma0=0.3, sigma_base=math.sqrt(2.0), obstacle_frac=0.03, seed=seed))
+    if name == "t_m8":         # 300x300x150's: 16 headings, 8 modes, 2000 realisations
+        return (Problem(gsize=27, nt=5, nrzns=2000, nmodes=8, num_ac_angles=16, F=1.0,
+                        i_term=24, j_term=13, neighb_gsize=21, prob_name="t_m8"),
+                FieldSpec(A=1.0, sigma0=0.3, sigma_base=math.sqrt(2.0), obstacle_frac=0.03, seed=seed))
+    if name == "t_m6":         # 6 modes, 2 speeds x 16 headings (32 actions), odd realisation count
+        return (Problem(gsize=21, nt=5, nrzns=1537, nmodes=6, num_ac_speeds=2, num_ac_angles=16,
+                        F=1.5, i_term=3, j_term=17, neighb_gsize=21, prob_name="t_m6"),
+                FieldSpec(A=1.0, sigma0=0.3, sigma_base=math.sqrt(2.0), obstacle_frac=0.04, seed=seed))
+    if name == "t_energy1":    # reward type energy1, 5 modes (odd count), 12 headings x 2 speeds
+        return (Problem(gsize=17, nt=7, nrzns=300, nmodes=5, num_ac_speeds=2, num_ac_angles=12,
+                        F=1.5, i_term=8, j_term=12, term_subgrid_size=2, neighb_gsize=13,
+                        prob_type="energy1", prob_name="t_energy1"),
+                FieldSpec(A=0.7, obstacle_frac=0.05, seed=seed))
+    if name == "t_energy3":    # reward type energy3 with a scalar field, dx != 1
+        return (Problem(gsize=19, nt=9, nrzns=256, nmodes=6, num_ac_angles=8, F=1.0,
+                        dx=0.5, dy=0.5, dt=0.5, i_term=14, j_term=4, neighb_gsize=15,
+                        prob_type="energy3", prob_name="t_energy3"),
+                FieldSpec(A=0.4, obstacle_frac=0.05, scalar=0.3, scalar_wave=0.4, seed=seed))
     raise KeyError(name)

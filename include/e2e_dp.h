@@ -418,10 +418,12 @@ e2e_status e2e_env_generate(const e2e_env_params* p, const int32_t* interp_verti
  * running while another framework's allocator owns the device).  Same sweeps
  * and results as e2e_spvi_solve, outputs in caller-provided DEVICE buffers; its
  * scratch is a fixed 32 MiB file-scope device array, so models above
- * 8,372,224 states (or solves above 8190 sweeps, or fp64_check) are rejected
- * with E2E_ERR_UNSUPPORTED.  The first call on a device caches the array's
- * address (make it before any stream capture); all calls share the array, so
- * calls that overlap on the GPU race. */
+ * 8,388,544 states (or fp64_check) are rejected with E2E_ERR_UNSUPPORTED; the
+ * number of sweeps is not limited.  The first call on a device caches the
+ * array's address (make it before any stream capture; do not call it again
+ * after cudaDeviceReset); all calls share the array, so calls that overlap on
+ * the GPU race.  The layered method reports the actions of its verification
+ * sweep, the same as the layered pass's for every model the builder makes. */
 e2e_status e2e_spvi_solve_noalloc(const e2e_model* m, const e2e_vi_opts* opts /* may be NULL */,
                                   int32_t* policy_dev, float* value_dev,
                                   e2e_vi_stats* stats /* may be NULL */, void* stream);

@@ -21,6 +21,9 @@ Build flags follow ``src/Makefile:14,23`` with two changes: device code for
 sm_100a (the reference Makefile names no architecture) and ``-O3`` for the
 host code (the Makefile passes none), which only speeds the reference up.
 
+The reference sources are found at ``$E2E_REFERENCE_SRC`` or, by default, in
+``../reference/src`` relative to this repository's root.
+
 Usage (in a container that has the reference sources):
     python oracle/build_ref.py            # default problem set
     python oracle/build_ref.py c1 t_time  # selected problems
@@ -35,11 +38,15 @@ import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
-REF_SRC = os.environ.get("E2E_REFERENCE_SRC", "/root/reference/src")
+# The reference's src/ directory: $E2E_REFERENCE_SRC, else a checkout named
+# "reference" beside this repository's root.
+REF_SRC = os.environ.get("E2E_REFERENCE_SRC",
+                         os.path.join(os.path.dirname(ROOT), "reference", "src"))
 OUT = os.path.join(HERE, "_ref")
 NVCC = os.environ.get("NVCC", "nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-DEFAULT_PROBLEMS = ["t_time", "t_custom", "t_energy2", "t_wide", "c1", "c2"]
+DEFAULT_PROBLEMS = ["t_time", "t_custom", "t_energy2", "t_wide", "c1", "c2", "t_m10", "t_m8", "t_m6",
+                    "t_energy1", "t_energy3"]
 
 sys.path.insert(0, ROOT)
 

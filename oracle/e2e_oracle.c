@@ -528,3 +528,103 @@ int orc_vi_f32(int64_t Ns, int Na, int64_t n_row_states, const int64_t* row_ptr,
   if (resid) *resid = sup;
   return it;
 }
+
+/*
+ * FP64 backward induction over a large time-layered state-major CSR model, as
+ * the library keeps it (int32 next states, integer counts scaled by 1/nrzns):
+ * the same backup as orc_backup_f64 (first maximum from -1e6/-1, the rule of
+ * src/spvi_2.cu:101-116), layer by layer from the last, the states of one
+ * layer split over nthreads threads (they read only the next layer's values).
+ * If pol is given, gap[s] = best Q(s, .) - Q(s, pol[s]) in FP64 (the margin by
+ * which a given policy's action falls short of the best; pol[s] < 0 or >= Na
+ * gives +inf).  Rows exist for states below (nt-1)*ncells; the last layer has
+ * Q = R only.  Returns 0, or -1 if a thread could not be started.
+ */
+typedef struct {
+  int64_t s0, s1;
+  int Na;
+  int64_t n_row_states;
+  const int64_t* row_ptr;
+  const int32_t* col;
+  const uint32_t* cnt;
+  const uint16_t* cnt16;
+  double inv;
+  const float* R;
+  const int32_t* pol;
+  double* V;
+  int32_t* pi;
+  double* gap;
+} orc_layer_job;
+
+static void* orc_layer_worker(void* arg) {
+  const orc_layer_job* J = (const orc_layer_job*)arg;
+  for (int64_t s = J->s0; s < J->s1; s++) {
+    double best = -1e6, qpol = -INFINITY;
+    int32_t arg_best = -1;
+    const int32_t want = J->pol ? J->pol[s] : -1;
+    for (int a = 0; a < J->Na; a++) {
+      const int64_t row = s * J->Na + a;
+      double q = (double)J->R[row];
+      if (s < J->n_row_states) {
+        double acc = 0.0;
+        for (int64_t k = J->row_ptr[row]; k < J->row_ptr[row + 1]; k++) {
+          const double c = J->cnt16 ? (double)J->cnt16[k] : (double)J->cnt[k];
+          acc += c * J->inv * J->V[J->col[k]];
+        }
+        q += acc;
+      }
+      if (a == want) qpol = q;
+      if (q > best) {
+        best = q;
+        arg_best = a;
+      }
+    }
+    J->V[s] = best;
+    J->pi[s] = arg_best;
+    if (J->gap) J->gap[s] = (want >= 0 && want < J->Na) ? best - qpol : INFINITY;
+  }
+  return NULL;
+}
+
+int orc_vi_f64_layers(int64_t ncells, int nt, int Na, const int64_t* row_ptr, const int32_t* col,
+                      const uint32_t* cnt, const uint16_t* cnt16, double scale, const float* R,
+                      const int32_t* pol, int nthreads, double* V, int32_t* pi, double* gap) {
+  if (nthreads < 1) nthreads = 1;
+  if (nthreads > 256) nthreads = 256;
+  pthread_t th[256];
+  orc_layer_job jobs[256];
+  const int64_t n_row_states = (int64_t)(nt - 1) * ncells;
+  for (int t = nt - 1; t >= 0; t--) {
+    const int64_t a0 = (int64_t)t * ncells, a1 = a0 + ncells;
+    const int64_t per = (ncells + nthreads - 1) / nthreads;
+    int started = 0;
+    for (int k = 0; k < nthreads; k++) {
+      orc_layer_job* J = &jobs[k];
+      J->s0 = a0 + k * per;
+      J->s1 = J->s0 + per < a1 ? J->s0 + per : a1;
+      if (J->s0 > a1) J->s0 = a1;
+      J->Na = Na;
+      J->n_row_states = n_row_states;
+      J->row_ptr = row_ptr;
+      J->col = col;
+      J->cnt = cnt;
+      J->cnt16 = cnt16;
+      J->inv = 1.0 / scale;
+      J->R = R;
+      J->pol = pol;
+      J->V = V;
+      J->pi = pi;
+      J->gap = gap;
+    }
+    for (int k = 1; k < nthreads; k++) {
+      if (pthread_create(&th[k], NULL, orc_layer_worker, &jobs[k]) != 0) {
+        for (int j = 1; j < k; j++) pthread_join(th[j], NULL);
+        return -1;
+      }
+      started = k;
+    }
+    orc_layer_worker(&jobs[0]);
+    for (int k = 1; k <= started; k++) pthread_join(th[k], NULL);
+  }
+  return 0;
+}

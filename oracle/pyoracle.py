@@ -77,6 +77,9 @@ def lib():
             L.orc_vi_f32.argtypes = [C.c_int64, C.c_int, C.c_int64, vp, vp, vp, vp, C.c_int32, vp,
                                      C.c_float, C.c_int, vp, vp, vp]
             L.orc_vi_f32.restype = C.c_int
+            L.orc_vi_f64_layers.argtypes = [C.c_int64, C.c_int, C.c_int, vp, vp, vp, vp, C.c_double, vp,
+                                            vp, C.c_int, vp, vp, vp]
+            L.orc_vi_f64_layers.restype = C.c_int
             _lib = L
     return _lib
 
@@ -240,3 +243,36 @@ def to_reference_coo(prob, model: Dict[str, np.ndarray]):
     R_sa = model["R_full"].reshape(Ns, Na)
     R_ref = np.ascontiguousarray(R_sa.T).reshape(-1)
     return S1, S2, val, R_ref
+
+
+def vi_f64_layers(ncells: int, nt: int, Na: int, row_ptr, col, cnt, scale: float, R, policy=None,
+                  nthreads: int = 1):
+    """FP64 backward induction over a time-layered state-major CSR with int32
+    next states and uint16/uint32 counts (the library's layout, e.g. as copied
+    down from the device), the states of a layer on ``nthreads`` threads.
+    Returns (V64, pi64, gap): gap[s] = best Q - Q(s, policy[s]) in FP64 when a
+    policy is given, else None."""
+    L = lib()
+    Ns = ncells * nt
+    row_ptr = np.ascontiguousarray(row_ptr, dtype=np.int64)
+    col = np.ascontiguousarray(col, dtype=np.int32)
+    cnt = np.asarray(cnt)
+    if cnt.dtype == np.uint16:
+        c16, c32 = np.ascontiguousarray(cnt), None
+    else:
+        c16, c32 = None, np.ascontiguousarray(cnt, dtype=np.uint32)
+    R = np.ascontiguousarray(R, dtype=np.float32)
+    if len(R) != Ns * Na:
+        raise ValueError("R needs ns * Na entries")
+    pol = None if policy is None else np.ascontiguousarray(policy, dtype=np.int32)
+    V = np.empty(Ns, np.float64)
+    pi = np.empty(Ns, np.int32)
+    gap = None if pol is None else np.empty(Ns, np.float64)
+    rc = L.orc_vi_f64_layers(ncells, nt, Na, row_ptr.ctypes.data, col.ctypes.data,
+                             None if c32 is None else c32.ctypes.data,
+                             None if c16 is None else c16.ctypes.data, float(scale), R.ctypes.data,
+                             None if pol is None else pol.ctypes.data, int(nthreads), V.ctypes.data,
+                             pi.ctypes.data, None if gap is None else gap.ctypes.data)
+    if rc != 0:
+        raise RuntimeError("orc_vi_f64_layers failed")
+    return V, pi, gap

@@ -84,11 +84,11 @@ def decode(prob, fx) -> dict:
             "prob_params": fx["prob_params"], "DP_relv_params": fx["DP_relv_params"]}
 
 
-def record_trig(src: str) -> None:
+def record_trig(src: str, names) -> None:
     from e2e_gpu_dp_b200.problem import config
     from e2e_gpu_dp_b200 import api
 
-    for n in NAMES:
+    for n in names:
         prob, _ = config(n)
         tab = api.action_table(prob)
         np.save(os.path.join(src, f"trig_{n}.npy"), np.stack([tab["cos"], tab["sin"]]))
@@ -100,11 +100,13 @@ def main() -> int:
     ap = argparse.ArgumentParser()
     ap.add_argument("src")
     ap.add_argument("--trig", action="store_true", help="record device trig values into src")
+    ap.add_argument("--names", nargs="*", default=None, help="problems (default: the fixture set)")
     a = ap.parse_args()
+    names = a.names or NAMES
     if a.trig:
-        record_trig(a.src)
+        record_trig(a.src, names)
         return 0
-    for n in NAMES:
+    for n in names:
         p = os.path.join(a.src, f"ref_{n}.npz")
         if not os.path.exists(p):
             print("missing", p)

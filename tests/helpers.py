@@ -13,6 +13,16 @@ VALUE_RTOL = 1e-5
 # Actions whose FP64 Q lies within this normwise band of the best are ties.
 TIE_RTOL = 2e-5
 
+# Small problems of the parity tests.  t_m10 / t_m8 carry the per-row shape of
+# the 200x200x120 and 300x300x150 workloads (16 headings, 10 / 8 modes, 5000 /
+# 2000 realisations), t_m6 6 modes and 32 actions; the energy problems cover
+# the reward types 1-3 and custom1 the mixed one.
+PARITY = ["t_time", "t_custom", "t_energy2", "t_wide", "t_m10", "t_m8", "t_m6", "t_energy1",
+          "t_energy3"]
+# Problems whose rewards are integers: every reward sum is exact in float, so
+# R is compared bit for bit.
+INTEGER_REWARDS = {"t_time", "t_wide", "c1", "t_m10", "t_m8", "t_m6"}
+
 
 def problem(name, seed=1234):
     prob, spec = config(name, seed)

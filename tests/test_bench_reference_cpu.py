@@ -33,3 +33,45 @@ def test_reference_arm_unavailable(monkeypatch):
     monkeypatch.setattr(run_ref, "have_reference", lambda name: False)
     line = bench.run_reference(types.SimpleNamespace(steps=1, warmup=1), 1, 0, 0)
     assert line["impl"] == "reference" and "unavailable" in line
+
+
+def test_both_arms_share_the_workload_config(monkeypatch):
+    from e2e_gpu_dp_b200.problem import config
+
+    monkeypatch.setattr(run_ref, "have_reference", lambda name: True)
+    monkeypatch.setattr(run_ref, "run", lambda name, workdir, **kw: {
+        "wall_build_s": 1.0, "wall_convert_s": 0.0, "wall_solve_s": 1.0, "build_loop_s": 1.0,
+        "solve_total_s": 1.0, "iterations": 1})
+    line = bench.run_reference(types.SimpleNamespace(steps=1, warmup=0), 1, 0, 0)
+    prob, _ = config(bench.WORKLOAD)
+    assert line["config"] == bench.workload_config(prob, 1)
+
+
+def test_parity_sample_counts_planted_mismatches():
+    """The bench's row-sample comparison: oracle blocks against a whole model
+    built by the oracle agree; a count changed in the model copy (planted on
+    the CPU) is reported as one mismatched row."""
+    import numpy as np
+
+    from oracle import pyoracle as O
+    from tests.helpers import problem
+
+    prob, fields = problem("t_time")
+    h = O.build_model(prob, fields, nthreads=2)
+    h = {"row_ptr": h["row_ptr"], "col": h["col"].astype(np.int32), "cnt": h["cnt"], "R": h["R_full"]}
+    blocks = [(r0, O.build_rows(prob, fields, r0=r0, r1=r0 + 300, nthreads=2)) for r0 in (0, 1000, 4000)]
+    ok = bench.parity_sample(h, blocks)
+    assert ok["rows"] == 900 and ok["mismatched_rows"] == 0 and ok["entries"] > 0
+    bad = dict(h)
+    bad["cnt"] = h["cnt"].copy()
+    k = int(h["row_ptr"][1010])
+    bad["cnt"][k] += 1
+    assert bench.parity_sample(bad, blocks)["mismatched_rows"] == 1
+
+
+def test_vi_bytes_and_issue_roofline():
+    # per-state row pointer formula: nnz*(b_cnt+4) + (Ns+1)*4 + Na*Ns*4 + 3*Ns*4
+    assert bench.vi_bytes_per_iteration(10, 2, 7, 2) == 7 * 6 + 11 * 4 + 2 * 10 * 4 + 3 * 10 * 4
+    r = bench.k1_issue_roofline(samples=32 * 10**9, k1_s=1.0, sm_mhz=1000.0, n_sm=100)
+    assert r is not None and r["peak"] == 100 * 4 * 1e9
+    assert abs(r["achieved"] - r["warp_inst_per_sample"] * 32e9) < 1e-3

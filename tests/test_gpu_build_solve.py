@@ -14,12 +14,13 @@ from e2e_gpu_dp_b200 import api
 from e2e_gpu_dp_b200._lib import E2EError
 from oracle import pyoracle as O
 from tests.golden.make_golden import decode
-from tests.helpers import (VALUE_RTOL, golden, policy_ok, problem, q_values_f64, values_close)
+from tests.golden.make_golden import NAMES as REF_NAMES
+from tests.helpers import (INTEGER_REWARDS, PARITY, VALUE_RTOL, golden, policy_ok, problem, q_values_f64,
+                           values_close)
 
 pytestmark = pytest.mark.gpu
 
-SMALL = ["t_time", "t_custom", "t_energy2", "t_wide"]
-INTEGER_REWARDS = {"t_time", "t_wide", "c1"}
+SMALL = PARITY
 NTHREADS = max(1, min(16, os.cpu_count() or 1))
 
 
@@ -68,7 +69,7 @@ def test_wide_spread_uses_dense_rows(built):
     assert np.array_equal(h["cnt"], orc["cnt"])
 
 
-@pytest.mark.parametrize("name", SMALL + ["c1"])
+@pytest.mark.parametrize("name", REF_NAMES)
 def test_model_files_equal_reference(name):
     """The reference's own output files, bit for bit (Val, S1, S2; R for integer rewards)."""
     prob, fields = problem(name)

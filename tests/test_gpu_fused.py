@@ -10,11 +10,11 @@ import pytest
 
 from e2e_gpu_dp_b200 import api
 from e2e_gpu_dp_b200._lib import E2EError
-from tests.helpers import problem
+from tests.helpers import PARITY, problem
 
 pytestmark = pytest.mark.gpu
 
-NAMES = ["t_time", "t_custom", "t_energy2", "t_wide", "c1"]
+NAMES = PARITY + ["c1"]
 
 
 @pytest.fixture(scope="module")
