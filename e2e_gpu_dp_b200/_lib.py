@@ -183,6 +183,7 @@ SIGNATURES = {
     "e2e_server_add_field": (C.c_int, [C.c_void_p, C.POINTER(Problem), C.POINTER(Fields), C.c_int,
                                        C.POINTER(C.c_int32)]),
     "e2e_server_submit": (C.c_int, [C.c_void_p, C.POINTER(Request), C.POINTER(C.c_int64)]),
+    "e2e_server_cancel": (C.c_int, [C.c_void_p, C.c_int64]),
     "e2e_server_poll": (C.c_int, [C.c_void_p, C.POINTER(Result), C.c_int32, C.POINTER(C.c_int32),
                                   C.c_double]),
     "e2e_server_fetch": (C.c_int, [C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p, C.c_int]),

@@ -237,6 +237,11 @@ class Server:
         check(lib().e2e_server_submit(self._h, C.byref(r), C.byref(rid)))
         return rid.value
 
+    def cancel(self, request_id: int) -> None:
+        """Cancel a queued request (e2e_server_cancel); its result comes back
+        from poll() with status E2E_ERR_CANCELLED."""
+        check(lib().e2e_server_cancel(self._h, request_id))
+
     def poll(self, max_results: int = 1024, wait_s: float = 0.0):
         buf = (_lib.Result * max_results)()
         n = C.c_int32()

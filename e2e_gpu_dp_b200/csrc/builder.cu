@@ -377,11 +377,11 @@ __global__ void __launch_bounds__(1024) k_build_tiles(BuildArgs A) {
   masks[MASK_EDGE * nthr + tid] = edge;
   masks[MASK_TERM * nthr + tid] = term;
   masks[MASK_SLOW * nthr + tid] = slow;
-  // a warp takes the general loop if any of its rows can land on an edge,
-  // terminal or slow bin
-  const bool plain_row = (mode != MODE_WINDOW) || ((edge | term | slow) == 0);
-  const bool plain_warp = __all_sync(0xffffffffu, plain_row);
-  const float r_plain = tab[aa][0];
+  // Unit cell spacing: every window row is counted (rewards folded from the
+  // counters per bin); a warp whose windows reach the grid's edge ring also
+  // counts the clamps of move(), which only samples landing in edge bins can
+  // have.  Other spacings take the general loop (per-sample rewards).
+  const bool clamp_warp = __any_sync(0xffffffffu, mode == MODE_WINDOW && edge != 0);
 
   float sumR = 0.f;
   uint32_t n_drop = 0, n_misbin = 0;
@@ -390,29 +390,62 @@ __global__ void __launch_bounds__(1024) k_build_tiles(BuildArgs A) {
   float2* myvel = velw + cl * kVelStride;   // this lane's cell
   const int per = 1 << lanes_log2;         // lanes sharing a cell
   // constants of the sample loops, held in registers
-  const float xs0 = P.xs0, ysn = P.ysn, axmax = P.axmax, aymax = P.aymax;
+  const float xs0 = P.xs0, ysn = P.ysn;
   const float xsn = P.xsn, ys0 = P.ys0, dt = P.dt, r_out = P.r_out;
-  const int kx = 0x4B400000 + wj0;  // float bits of 1.5*2^23 plus the window origin:
-  const int ky = 0x4B400000 + wi0;  // round_half_up_index then gives window-local indices
   // the same constants as (x, y) pairs for the packed float2 instructions
   const float2 FF = make_float2(F, F), csn = make_float2(cs, sn), dt2 = make_float2(dt, dt);
   const float2 xy1 = make_float2(x1, y1);
   const float2 sgn = make_float2(1.0f, -1.0f), org = make_float2(-xs0, ysn);
   const bool y_pairs = (nm % 2 == 0) && ((reinterpret_cast<uintptr_t>(A.F.Y) & 7) == 0);
 
-  // In-window rewards of a plain row, from its counters: such a sample's
-  // reward is r_plain, or r_outbound in an obstacle-overridden bin, so the
-  // row's sum gains count x reward per bin kind instead of one addition per
-  // sample (the reference adds them with float atomics in no fixed order).
+  // Rewards of the counted (in-window) samples of a row, from its counters.
+  // Without a clamp a sample's reward depends only on its bin: r_outbound in an
+  // obstacle-overridden bin (src/build_model.cu:538-540), else move()'s edge,
+  // terminal and late-time terms plus the step reward (:312-354, :533; the
+  // scalar field at the bin for the radiation rewards), evaluated with the
+  // reference's float operations; each clamp adds one r_outbound more
+  // (:291-310), counted per sample in n_cl.  The row's sum gains count x
+  // reward per bin instead of one addition per sample (the reference adds its
+  // rewards with float atomics in no fixed order; for integer rewards every
+  // partial sum is exact).  Samples in bins outside the m x m neighbourhood
+  // are not counted by the reference (their rewards are): they are dropped here.
+  int n_cl = 0;
   auto fold_window = [&]() {
-    uint32_t n_pl = 0, n_ovr = 0;
+    const uint64_t m_edge = masks[MASK_EDGE * nthr + tid];
+    const uint64_t m_term = masks[MASK_TERM * nthr + tid];
+    const uint64_t m_in = masks[MASK_INWIN * nthr + tid];
     for (int wl = 0; wl < kWinBins; ++wl) {
-      const uint32_t w = wcol[wl << log2S];
-      if (w & kOvrFlag) n_ovr += w & kCountMask;
-      else n_pl += w;
+      uint16_t* p = wcol + (wl << log2S);
+      const uint32_t w = *p;
+      const uint32_t c = w & kCountMask;
+      if (!c) continue;
+      float r;
+      if (w & kOvrFlag) {
+        r = r_out;
+      } else {
+        const int k = bit64(m_edge, wl) ? 1 : 0;
+        const bool tm = bit64(m_term, wl);
+        if (!rad) {
+          r = tab[aa][(tm ? 4 : 0) + k];
+        } else {
+          const int i2 = wi0 + (wl >> 3), j2 = wj0 + (wl & 7);
+          const float rad2 = __ldg(A.F.s + (int64_t)(T + 1) * nc + (int64_t)i2 * g + j2);
+          r = k ? r_out : 0.f;
+          if (tm) r += P.r_term;
+          else if (late) r += 0.05 * P.r_out;
+          r += step_reward(P, F, rad1, rad2);
+        }
+      }
+      sumR += (float)c * r;
+      if (!bit64(m_in, wl)) {
+        n_drop += c;
+        const int i2 = wi0 + (wl >> 3), j2 = wj0 + (wl & 7);
+        if (i2 - i1 + P.del < P.m && j2 - j1 + P.del < P.m) n_misbin += c;
+        *p = (uint16_t)(w & kOvrFlag);
+      }
     }
-    sumR += (float)n_pl * r_plain;
-    sumR += (float)n_ovr * r_out;
+    sumR += (float)n_cl * r_out;
+    n_cl = 0;
   };
 
   // Full reference expression for one sample (rare): reward, counts, dense
@@ -442,7 +475,7 @@ __global__ void __launch_bounds__(1024) k_build_tiles(BuildArgs A) {
     if (di >= 0 && di < P.m && dj >= 0 && dj < P.m) {
       if (mode == MODE_WINDOW) {
         // switch this row to a dense m*m histogram from the pool
-        if (plain_warp) fold_window();  // the window's samples are final
+        if (UNIT) fold_window();  // the window's samples are final
         unsigned long long slot = atomicAdd(A.counters + CTR_POOL, 1ull);
         atomicAdd(A.counters + CTR_OVERFLOW_ROWS, 1ull);
         if (slot < (unsigned long long)A.pool_units) {
@@ -551,7 +584,7 @@ __global__ void __launch_bounds__(1024) k_build_tiles(BuildArgs A) {
       for (int q = 0; q < clen; ++q) sumR += r_fixed;
     } else if (mode == MODE_WINDOW) {
       int n_out = 0;
-      if (plain_warp) {
+      if (UNIT) {
         // counts only: the rewards are folded from the counters at the end, a
         // sample that leaves the window counts in the miss bin
         // The window origin is folded into the rounding constant: the bits of
@@ -565,25 +598,47 @@ __global__ void __launch_bounds__(1024) k_build_tiles(BuildArgs A) {
         const uint32_t sh = (uint32_t)log2S + 1u;  // bytes per bin row, log2
         const uint32_t base_adj = (uint32_t)__cvta_generic_to_shared(wcol) - ((9u * M) << sh);
         const uint32_t miss_idx = 9u * M + (uint32_t)kMissBin;
-        auto count_sample = [&](float2 vv) {
-          const float2 xy = advect2(FF, csn, vv, dt2, xy1);  // move(), src/build_model.cu:284-289
-          // (xnew - xs0, -(ynew - ysn)) without the domain clamps: a plain
-          // row's window holds no edge cell, so a sample the clamps would move
-          // lands outside the window either way (unclamped its index is below 0
-          // or above g-1; a NaN or a value beyond 2^22 gives bits far from
-          // 0x4B400000) and is taken again by the rescan below
+        // one sample: its window bin (or the miss bin) counter incremented;
+        // returns the counter's previous value and the landing position
+        auto bump = [&](float2 vv, float2& xy, bool& inw) -> uint32_t {
+          xy = advect2(FF, csn, vv, dt2, xy1);  // move(), src/build_model.cu:284-289
+          // (xnew - xs0, -(ynew - ysn)) without the domain clamps: a sample
+          // the clamps move lands in an edge bin either way (unclamped its
+          // index is the edge cell's, or beyond the grid and so outside the
+          // window; a NaN or a value beyond 2^22 gives bits far from
+          // 0x4B400000) and a sample outside the window is taken again by the
+          // rescan below
           const float2 d = __ffma2_rn(xy, sgn, org);
           const float2 w = __fadd2_rd(d, make_float2(0.5f, 0.5f));  // round_half_up_index
           const float2 t = __fadd2_rd(w, magic);
           const uint32_t bx = __float_as_uint(t.x), by = __float_as_uint(t.y);
-          const bool inw = ((bx ^ M) | (by ^ M)) < (uint32_t)kWin;
+          inw = ((bx ^ M) | (by ^ M)) < (uint32_t)kWin;
           const uint32_t addr = base_adj + ((inw ? (by << 3) + bx : miss_idx) << sh);
           unsigned short v;
           asm volatile("ld.shared.u16 %0, [%1];" : "=h"(v) : "r"(addr));
-          v = (unsigned short)(v + 1);
-          asm volatile("st.shared.u16 [%0], %1;" ::"r"(addr), "h"(v));
+          const unsigned short v1 = (unsigned short)(v + 1);
+          asm volatile("st.shared.u16 [%0], %1;" ::"r"(addr), "h"(v1));
+          return v;
         };
-        if constexpr (FUSED) {
+        auto count_sample = [&](float2 vv) {
+          float2 xy;
+          bool inw;
+          bump(vv, xy, inw);
+        };
+        // a warp whose windows hold edge bins: each clamp of an in-window
+        // sample outside an obstacle-overridden bin adds one r_outbound
+        auto count_sample_clamp = [&](float2 vv) {
+          float2 xy;
+          bool inw;
+          const uint32_t v = bump(vv, xy, inw);
+          const bool add = inw && !(v & kOvrFlag);
+          n_cl += (add && (xy.x > xsn || xy.x < xs0)) ? 1 : 0;
+          n_cl += (add && (xy.y > ysn || xy.y < ys0)) ? 1 : 0;
+        };
+        if (clamp_warp) {
+#pragma unroll 8
+          for (int q = 0; q < clen; ++q) count_sample_clamp(myvel[q]);
+        } else if constexpr (FUSED) {
           // one realisation a load: the fused instance measured 444 ms with
           // the pairs below and 419 ms without them (200x200x120)
 #pragma unroll 16
@@ -605,6 +660,8 @@ __global__ void __launch_bounds__(1024) k_build_tiles(BuildArgs A) {
         n_out = *mp;
         if (n_out) *mp = 0;
       } else {
+        // general cell spacing: the reference's remainderf snapping and a
+        // reward per sample
         const uint64_t m_edge = masks[MASK_EDGE * nthr + tid];
         const uint64_t m_term = masks[MASK_TERM * nthr + tid];
         const uint64_t m_slow = masks[MASK_SLOW * nthr + tid];
@@ -614,17 +671,9 @@ __global__ void __launch_bounds__(1024) k_build_tiles(BuildArgs A) {
           const float2 xy = advect2(FF, csn, vv, dt2, xy1);
           const float xnew = xy.x, ynew = xy.y;
           const int kcl = ((xnew > xsn) || (xnew < xs0) ? 1 : 0) + ((ynew > ysn) || (ynew < ys0) ? 1 : 0);
-          int li, lj;
-          if (UNIT) {
-            const float2 d = __ffma2_rn(xy, sgn, org);
-            const float2 ad = make_float2(fminf(fmaxf(d.x, 0.0f), axmax), fminf(fmaxf(d.y, 0.0f), aymax));
-            round_half_up_index2(ad, kx, ky, lj, li);
-          } else {
-            int i2, j2;
-            land<UNIT>(P, F, cs, sn, vv.x, vv.y, x1, y1, i2, j2);
-            li = i2 - wi0;
-            lj = j2 - wj0;
-          }
+          int i2, j2;
+          land<UNIT>(P, F, cs, sn, vv.x, vv.y, x1, y1, i2, j2);
+          const int li = i2 - wi0, lj = j2 - wj0;
           const bool inw = (unsigned)(li | lj) < (unsigned)kWin;
           const int b = inw ? (li << 3) + lj : 0;
           const bool fast = inw && !bit64(m_slow, b);
@@ -640,8 +689,9 @@ __global__ void __launch_bounds__(1024) k_build_tiles(BuildArgs A) {
         }
       }
       if (n_out) {
-        // rescan: the chunk's samples that left the window or hit a slow bin
-        const uint64_t m_slow = masks[MASK_SLOW * nthr + tid];
+        // rescan: the chunk's samples that left the window or (general loop)
+        // hit a slow bin
+        const uint64_t m_slow = UNIT ? 0ull : masks[MASK_SLOW * nthr + tid];
         for (int q = 0; q < clen; ++q) {
           const float2 vv = myvel[q];
           int i2, j2;
@@ -663,7 +713,7 @@ __global__ void __launch_bounds__(1024) k_build_tiles(BuildArgs A) {
       }
     }
   }
-  if (plain_warp && mode == MODE_WINDOW) fold_window();
+  if (UNIT && mode == MODE_WINDOW) fold_window();
   if (n_drop) atomicAdd(A.counters + CTR_DROPPED, (unsigned long long)n_drop);
   if (n_misbin) atomicAdd(A.counters + CTR_MISBIN, (unsigned long long)n_misbin);
   if (mode == MODE_LOST) atomicOr(reinterpret_cast<unsigned int*>(A.counters + CTR_FLAGS), FLAG_POOL_EXHAUSTED);

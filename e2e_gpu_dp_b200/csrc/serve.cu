@@ -535,6 +535,35 @@ extern "C" e2e_status e2e_server_submit(e2e_server* srv, const e2e_request* r, i
   return E2E_OK;
 }
 
+extern "C" e2e_status e2e_server_cancel(e2e_server* srv, int64_t request_id) {
+  using namespace e2e;
+  auto* S = reinterpret_cast<Server*>(srv);
+  if (!S) return fail(E2E_ERR_INVALID, "null server");
+  {
+    std::lock_guard<std::mutex> lk(S->mu);
+    for (auto it = S->pending.begin(); it != S->pending.end(); ++it) {
+      Req* q = *it;
+      if (q->id != request_id) continue;
+      // still queued: it holds no device memory (outputs are allocated when a
+      // batch takes it), so it leaves the queue with its result at once
+      S->pending.erase(it);
+      q->res.request_id = q->id;
+      q->res.tag = q->r.tag;
+      q->res.status = E2E_ERR_CANCELLED;
+      q->res.latency_ms = std::chrono::duration<double, std::milli>(Clock::now() - q->submit).count();
+      q->res.queue_ms = q->res.latency_ms;
+      S->done.push_back(q->res);
+      ++S->n_done;
+      ++S->n_failed;
+      delete q;
+      S->cv_done.notify_all();
+      return E2E_OK;
+    }
+    if (request_id <= 0 || request_id >= S->next_id) return fail(E2E_ERR_INVALID, "unknown request id");
+  }
+  return fail(E2E_ERR_BUSY, "request already taken into a batch or finished; it completes normally");
+}
+
 extern "C" e2e_status e2e_server_poll(e2e_server* srv, e2e_result* out, int32_t max, int32_t* n_out,
                                       double wait_s) {
   using namespace e2e;

@@ -33,6 +33,7 @@
 #include <math.h>
 
 #include <algorithm>
+#include <cstdlib>
 #include <type_traits>
 
 #include "internal.h"
@@ -47,6 +48,30 @@ constexpr int PF_NEXT = VI_TUNE_PF_NEXT;
 constexpr int PF_CURRENT = VI_TUNE_PF_CURRENT;
 constexpr long long kBarrierSpinLimit = 1ll << 22;
 constexpr unsigned long long kBarrierTimeoutNs = 2000000000ull;  // 2 s
+
+// Bounds of the device-side waits of the persistent sweeps (grid barriers of
+// the layered sweep, per-layer completion counters of the batched sweep): a
+// wait gives up after `spins` polls or `timeout_ns`, sets an error bit the
+// host reads (E2E_ERR_DEVICE) and lets the launch drain.  `extra` raises every
+// wait's target so that no wait can complete: the test hook that makes the
+// bounded waits run out on purpose, without any fault.
+struct WaitBound {
+  unsigned long long timeout_ns;
+  long long spins;
+  unsigned int extra;
+};
+
+// Host: E2E_WAIT_LIMIT_MS (default 2000) bounds each wait; with
+// E2E_TEST_UNREACHABLE_WAIT=1 the targets are raised by one (tests only).
+WaitBound wait_bound_from_env() {
+  WaitBound w{kBarrierTimeoutNs, kBarrierSpinLimit, 0u};
+  if (const char* ms = std::getenv("E2E_WAIT_LIMIT_MS")) {
+    const double v = std::atof(ms);
+    if (v > 0 && v <= 60000) w.timeout_ns = (unsigned long long)(v * 1e6);
+  }
+  if (const char* u = std::getenv("E2E_TEST_UNREACHABLE_WAIT")) w.extra = (u[0] == '1') ? 1u : 0u;
+  return w;
+}
 
 __device__ __forceinline__ void prefetch_l2(const void* p, uint32_t bytes) {
   // bulk prefetch into L2: no shared memory, no completion to wait for
@@ -526,7 +551,7 @@ __global__ void __launch_bounds__(kThreads)
 // Grid-wide barrier of a cooperative launch.  sync[0] counts arrivals (never
 // reset inside a launch); a wait that outlives its limit sets bit 1 of sync[1]
 // and every later barrier returns false at once.
-__device__ __forceinline__ bool grid_barrier(unsigned int* sync, unsigned int target) {
+__device__ __forceinline__ bool grid_barrier(unsigned int* sync, unsigned int target, const WaitBound& wb) {
   __shared__ int ok;
   __syncthreads();
   if (threadIdx.x == 0) {
@@ -535,8 +560,8 @@ __device__ __forceinline__ bool grid_barrier(unsigned int* sync, unsigned int ta
     atomicAdd(sync, 1u);
     const unsigned long long t0 = global_ns();
     long long it = 0;
-    while (ld_acquire(sync) < target) {
-      if (ld_acquire(sync + 1) != 0u || ++it > kBarrierSpinLimit || global_ns() - t0 > kBarrierTimeoutNs) {
+    while (ld_acquire(sync) < target + wb.extra) {
+      if (ld_acquire(sync + 1) != 0u || ++it > wb.spins || global_ns() - t0 > wb.timeout_ns) {
         atomicOr(sync + 1, 2u);
         good = 0;
         break;
@@ -559,7 +584,7 @@ __device__ __forceinline__ bool grid_barrier(unsigned int* sync, unsigned int ta
 // work, so HBM streams layer t-1 while layer t computes.
 template <int MODE, typename CntT, int VAR>
 __global__ void __launch_bounds__(kThreads, MinBlocks<MODE, VAR>::value)
-    k_vi_layered(ViPack P, int groups, float* V, int32_t* pi, unsigned int* sync, int prefetch) {
+    k_vi_layered(ViPack P, int groups, float* V, int32_t* pi, unsigned int* sync, int prefetch, WaitBound wb) {
   __shared__ float sq[kWarps][32];
   __shared__ int sa[kWarps][32];
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
@@ -608,7 +633,7 @@ __global__ void __launch_bounds__(kThreads, MinBlocks<MODE, VAR>::value)
     }
     if (t > 0) {
       ++gen;
-      if (!grid_barrier(sync, gen * gridDim.x)) return;
+      if (!grid_barrier(sync, gen * gridDim.x, wb)) return;
     }
   }
 }
@@ -635,7 +660,7 @@ struct BatchMinBlocks {  // the job lookup needs a few more registers than k_vi_
 template <int MODE, typename CntT, int VAR>
 __global__ void __launch_bounds__(kThreads, BatchMinBlocks<MODE, VAR>::value)
     k_vi_batch(const unsigned char* table, int job_cap, int groups, int* done, int layer_cap,
-               unsigned int* err, int prefetch) {
+               unsigned int* err, int prefetch, WaitBound wb) {
   __shared__ float sq[kWarps][32];
   __shared__ int sa[kWarps][32];
   const ViBatchHeader* H = reinterpret_cast<const ViBatchHeader*>(table);
@@ -685,8 +710,8 @@ __global__ void __launch_bounds__(kThreads, BatchMinBlocks<MODE, VAR>::value)
           if (lane == 0) {
             const unsigned long long t0 = global_ns();
             long long it = 0;
-            while (ld_acquire_s32(dep) < cpl) {
-              if (ld_acquire(err) != 0u || ++it > kBarrierSpinLimit || global_ns() - t0 > kBarrierTimeoutNs) {
+            while (ld_acquire_s32(dep) < cpl + (int)wb.extra) {
+              if (ld_acquire(err) != 0u || ++it > wb.spins || global_ns() - t0 > wb.timeout_ns) {
                 atomicOr(err, 4u);
                 ok = 0;
                 break;
@@ -1067,7 +1092,8 @@ cudaError_t launch_vi_layered(const ViPack& P, float* V, int32_t* pi, unsigned i
     if (grid < 1) grid = 1;
     ViPack Pc = P;
     int pf = prefetch;
-    void* args[] = {(void*)&Pc, (void*)&G, (void*)&V, (void*)&pi, (void*)&sync, (void*)&pf};
+    WaitBound wb = wait_bound_from_env();
+    void* args[] = {(void*)&Pc, (void*)&G, (void*)&V, (void*)&pi, (void*)&sync, (void*)&pf, (void*)&wb};
     return cudaLaunchCooperativeKernel((const void*)kern, dim3((unsigned)grid), dim3(kThreads), args, 0, st);
   });
 }
@@ -1126,7 +1152,8 @@ cudaError_t launch_vi_batch(const void* table, int job_cap, int layer_cap, int e
     cfg.numAttrs = 1;
     const unsigned char* tb = reinterpret_cast<const unsigned char*>(table);
     int pf = prefetch;
-    return cudaLaunchKernelEx(&cfg, kern, tb, job_cap, groups, done, layer_cap, err, pf);
+    const WaitBound wb = wait_bound_from_env();
+    return cudaLaunchKernelEx(&cfg, kern, tb, job_cap, groups, done, layer_cap, err, pf, wb);
   });
 }
 

@@ -379,6 +379,11 @@ def config(name: str, seed: int = 1234) -> Tuple[Problem, FieldSpec]:
                         F=1.5, i_term=8, j_term=12, term_subgrid_size=2, neighb_gsize=13,
                         prob_type="energy1", prob_name="t_energy1"),
                 FieldSpec(A=0.7, obstacle_frac=0.05, seed=seed))
+    if name == "t_half":       # time reward with half-cell spacing: remainderf snapping, no scalar field
+        return (Problem(gsize=20, nt=7, nrzns=200, nmodes=4, num_ac_angles=16, F=1.0,
+                        dx=0.5, dy=0.5, dt=0.5, i_term=6, j_term=15, neighb_gsize=13,
+                        prob_name="t_half"),
+                FieldSpec(A=0.5, sigma0=0.25, obstacle_frac=0.04, seed=seed))
     if name == "t_energy3":    # reward type energy3 with a scalar field, dx != 1
         return (Problem(gsize=19, nt=9, nrzns=256, nmodes=6, num_ac_angles=8, F=1.0,
                         dx=0.5, dy=0.5, dt=0.5, i_term=14, j_term=4, neighb_gsize=15,

@@ -304,6 +304,12 @@ e2e_status e2e_server_create(const e2e_server_opts* opts /* may be NULL */, e2e_
 e2e_status e2e_server_add_field(e2e_server* s, const e2e_problem* p, const e2e_fields* f, int fields_where,
                                 int32_t* field_id);
 e2e_status e2e_server_submit(e2e_server* s, const e2e_request* r, int64_t* request_id);
+/* Cancel a request that is still queued: its result (status E2E_ERR_CANCELLED)
+ * is returned by e2e_server_poll.  E2E_ERR_BUSY if a batch has already taken it
+ * (it completes normally), E2E_ERR_INVALID for an unknown id.  No counterpart in
+ * the reference (whose solver declares a timeout status it never sets,
+ * src/spvi_2.cu:650-726). */
+e2e_status e2e_server_cancel(e2e_server* s, int64_t request_id);
 /* up to max finished results; waits up to wait_s seconds when none is ready */
 e2e_status e2e_server_poll(e2e_server* s, e2e_result* out, int32_t max, int32_t* n_out, double wait_s);
 /* full value / policy (ns = nt * gsize^2 each) of a finished keep_outputs request */

@@ -45,7 +45,7 @@ REF_SRC = os.environ.get("E2E_REFERENCE_SRC",
 OUT = os.path.join(HERE, "_ref")
 NVCC = os.environ.get("NVCC", "nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-DEFAULT_PROBLEMS = ["t_time", "t_custom", "t_energy2", "t_wide", "c1", "c2", "t_m10", "t_m8", "t_m6",
+DEFAULT_PROBLEMS = ["t_time", "t_custom", "t_energy2", "t_wide", "c1", "c2", "t_m10", "t_m8", "t_m6", "t_half",
                     "t_energy1", "t_energy3"]
 
 sys.path.insert(0, ROOT)

@@ -18,10 +18,11 @@ TIE_RTOL = 2e-5
 # 2000 realisations), t_m6 6 modes and 32 actions; the energy problems cover
 # the reward types 1-3 and custom1 the mixed one.
 PARITY = ["t_time", "t_custom", "t_energy2", "t_wide", "t_m10", "t_m8", "t_m6", "t_energy1",
-          "t_energy3"]
+          "t_energy3", "t_half"]
 # Problems whose rewards are integers: every reward sum is exact in float, so
-# R is compared bit for bit.
-INTEGER_REWARDS = {"t_time", "t_wide", "c1", "t_m10", "t_m8", "t_m6"}
+# R is compared bit for bit (t_half's time step is 0.5: sums of halves and
+# hundreds, exact too).
+INTEGER_REWARDS = {"t_time", "t_wide", "c1", "t_m10", "t_m8", "t_m6", "t_half"}
 
 
 def problem(name, seed=1234):
