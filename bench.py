@@ -748,8 +748,11 @@ def run_served(rates=(50, 200, 500, 1000, 2000), seconds_per_rate=10.0, max_requ
     fids = [srv.add_field(fc.prob, f) for fc, f in zip(fcs, dev)]
     assert fids == list(range(len(fcs)))
 
-    def serve(reqs, paced=True):
+    large_fids = {fc.fid for fc in fcs if fc.prob.gsize >= 300}
+
+    def serve(reqs, paced=True, srv=srv):
         lat, qd, bs = [], [], []
+        lat_small, lat_large = [], []
         results = {}
 
         def submitter():
@@ -768,15 +771,23 @@ def run_served(rates=(50, 200, 500, 1000, 2000), seconds_per_rate=10.0, max_requ
                 results[res["tag"]] = res
         t1 = time.perf_counter()
         th.join()
-        for res in results.values():
+        for k, res in results.items():
             lat.append(res["latency_ms"])
             qd.append(res["queue_ms"])
             bs.append(res["batch_size"])
+            (lat_large if reqs[k].fid in large_fids else lat_small).append(res["latency_ms"])
         fails = sum(1 for res in results.values() if res["status"] != 0)
+
+        def pct(x, q):
+            return round(float(np.percentile(x, q)), 3) if x else None
+
         return results, {"requests": len(reqs), "failed": fails, "seconds": round(t1 - t0, 4),
                          "solves_per_s": round(len(reqs) / (t1 - t0), 1),
-                         "p50_ms": round(float(np.percentile(lat, 50)), 3),
-                         "p99_ms": round(float(np.percentile(lat, 99)), 3),
+                         "p50_ms": pct(lat, 50), "p99_ms": pct(lat, 99),
+                         "small": {"requests": len(lat_small), "p50_ms": pct(lat_small, 50),
+                                   "p99_ms": pct(lat_small, 99)},
+                         "large_300x300x150": {"requests": len(lat_large), "p50_ms": pct(lat_large, 50),
+                                               "p99_ms": pct(lat_large, 99)},
                          "mean_queue_ms": round(float(np.mean(qd)), 3),
                          "mean_batch": round(float(np.mean(bs)), 1), "max_batch": int(np.max(bs))}
 
@@ -796,6 +807,7 @@ def run_served(rates=(50, 200, 500, 1000, 2000), seconds_per_rate=10.0, max_requ
     burst_reqs = request_stream(fcs, 5000, 1e9, seed=99)
     burst_res, burst = serve(burst_reqs, paced=False)
 
+
     # plain path on a sample of the burst's requests, one at a time
     sample = burst_reqs[:plain_sample]
     plain_lat, err = [], 0.0
@@ -814,6 +826,20 @@ def run_served(rates=(50, 200, 500, 1000, 2000), seconds_per_rate=10.0, max_requ
     plain_s = time.perf_counter() - tp0
     st = srv.stats()
     srv.close()
+    # the same server design without batching: one request per launch, every
+    # base model cached as above (isolates continuous batching from caching)
+    one = api.Server(max_batch=1)
+    for fc, f in zip(fcs, dev):
+        one.add_field(fc.prob, f)
+    serve(warm, paced=False, srv=one)
+    _, one_burst = serve(burst_reqs[:2000], paced=False, srv=one)
+    one_rates = []
+    for lam in (1000, 2000):
+        reqs = request_stream(fcs, int(min(max_requests, lam * seconds_per_rate)), lam, seed=int(lam))
+        _, st1 = serve(reqs, srv=one)
+        st1["rate"] = lam
+        one_rates.append(st1)
+    one.close()
     plain_rate = len(sample) / plain_s
     return {
         "workload": "16 resident fields (15 of grid 32-160, nt 20-100, nrzns 200-2000, 4-8 modes; one "
@@ -824,7 +850,10 @@ def run_served(rates=(50, 200, 500, 1000, 2000), seconds_per_rate=10.0, max_requ
         "plain": {"sample": len(sample), "solves_per_s": round(plain_rate, 2),
                   "p50_ms": round(float(np.percentile(plain_lat, 50)), 3),
                   "p99_ms": round(float(np.percentile(plain_lat, 99)), 3)},
+        "unbatched_server": {"max_batch": 1, "burst": one_burst, "rates": one_rates,
+                             "note": "same server, cached base models, one request per launch"},
         "speedup_vs_plain_burst": round(burst["solves_per_s"] / plain_rate, 1),
+        "batching_speedup_burst": round(burst["solves_per_s"] / one_burst["solves_per_s"], 2),
         "speedup_vs_plain_at_2000": round(per_rate[-1]["solves_per_s"] / plain_rate, 1),
         "max_rel_value_err_vs_plain": err,
         "server": {"batches": st["batches"], "models_built": st["models_built"],
