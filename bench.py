@@ -299,28 +299,43 @@ def cpu_baseline(prob, fields, threads: int, target_s: float = 15.0, trig=None):
 
 
 def parity_sample(h, blocks, integer_rewards: bool = True) -> dict:
-    """Device rows against the oracle's rows of the same blocks: row lengths,
-    next states and counts bit for bit, rewards bit for bit (integer rewards)."""
+    """Device rows against the oracle's rows of the same blocks: each row's
+    length, next states and counts bit for bit, rewards bit for bit (integer
+    rewards).  Rows are compared one by one (a differing row does not shift
+    the comparison of the rows after it)."""
     rows = entries = bad_rows = 0
     for r0, o in blocks:
         n = len(o["row_ptr"]) - 1
         rp = h["row_ptr"][r0:r0 + n + 1].astype(np.int64)
-        e0, e1 = int(rp[0]), int(rp[-1])
-        col, cnt = h["col"][e0:e1].astype(np.int64), h["cnt"][e0:e1].astype(np.int64)
         orp = o["row_ptr"].astype(np.int64)
-        same_len = (rp - rp[0]) == (orp - orp[0])
-        if np.all(same_len):
-            diff = (col != o["col"].astype(np.int64)) | (cnt != o["cnt"].astype(np.int64))
-            bad = np.zeros(n, bool)
+        glen, olen = np.diff(rp), np.diff(orp)
+        bad = glen != olen
+        same = np.nonzero(~bad)[0]
+        if len(same):
+            # entries of the rows of equal length, side by side
+            ln = glen[same]
+            g_idx = np.repeat(rp[:-1][same], ln) + _ranges(ln)
+            o_idx = np.repeat(orp[:-1][same] - orp[0], ln) + _ranges(ln)
+            diff = (h["col"][g_idx].astype(np.int64) != o["col"][o_idx].astype(np.int64)) | \
+                   (h["cnt"][g_idx].astype(np.int64) != o["cnt"][o_idx].astype(np.int64))
             if diff.any():
-                bad[np.searchsorted(orp[1:] - orp[0], np.nonzero(diff)[0], side="right")] = True
-        else:
-            bad = ~(same_len[1:] & same_len[:-1])
-        r_bad = h["R"][r0:r0 + n] != o["R"] if integer_rewards else np.zeros(n, bool)
-        bad_rows += int(np.sum(bad | r_bad))
+                bad[same[np.repeat(np.arange(len(same)), ln)[diff]]] = True
+        if integer_rewards:
+            bad |= h["R"][r0:r0 + n] != o["R"]
+        bad_rows += int(np.sum(bad))
         rows += n
         entries += len(o["col"])
     return {"rows": rows, "entries": entries, "mismatched_rows": bad_rows}
+
+
+def _ranges(lengths):
+    """0..l-1 for every l in lengths, concatenated."""
+    lengths = np.asarray(lengths, np.int64)
+    if len(lengths) == 0:
+        return np.zeros(0, np.int64)
+    tot = int(lengths.sum())
+    starts = np.repeat(np.cumsum(lengths) - lengths, lengths)
+    return np.arange(tot, dtype=np.int64) - starts
 
 
 def run_ours(args, ws, rank, local):

@@ -390,7 +390,7 @@ __global__ void __launch_bounds__(1024) k_build_tiles(BuildArgs A) {
   float2* myvel = velw + cl * kVelStride;   // this lane's cell
   const int per = 1 << lanes_log2;         // lanes sharing a cell
   // constants of the sample loops, held in registers
-  const float xs0 = P.xs0, ysn = P.ysn;
+  const float xs0 = P.xs0, ysn = P.ysn, axmax = P.axmax, aymax = P.aymax;
   const float xsn = P.xsn, ys0 = P.ys0, dt = P.dt, r_out = P.r_out;
   // the same constants as (x, y) pairs for the packed float2 instructions
   const float2 FF = make_float2(F, F), csn = make_float2(cs, sn), dt2 = make_float2(dt, dt);
@@ -598,17 +598,10 @@ __global__ void __launch_bounds__(1024) k_build_tiles(BuildArgs A) {
         const uint32_t sh = (uint32_t)log2S + 1u;  // bytes per bin row, log2
         const uint32_t base_adj = (uint32_t)__cvta_generic_to_shared(wcol) - ((9u * M) << sh);
         const uint32_t miss_idx = 9u * M + (uint32_t)kMissBin;
-        // one sample: its window bin (or the miss bin) counter incremented;
-        // returns the counter's previous value and the landing position
-        auto bump = [&](float2 vv, float2& xy, bool& inw) -> uint32_t {
-          xy = advect2(FF, csn, vv, dt2, xy1);  // move(), src/build_model.cu:284-289
-          // (xnew - xs0, -(ynew - ysn)) without the domain clamps: a sample
-          // the clamps move lands in an edge bin either way (unclamped its
-          // index is the edge cell's, or beyond the grid and so outside the
-          // window; a NaN or a value beyond 2^22 gives bits far from
-          // 0x4B400000) and a sample outside the window is taken again by the
-          // rescan below
-          const float2 d = __ffma2_rn(xy, sgn, org);
+        // one sample at window-relative snapping coordinates d: its window bin
+        // (or the miss bin) counter incremented; returns the counter's value
+        // before
+        auto bump = [&](float2 d, bool& inw) -> uint32_t {
           const float2 w = __fadd2_rd(d, make_float2(0.5f, 0.5f));  // round_half_up_index
           const float2 t = __fadd2_rd(w, magic);
           const uint32_t bx = __float_as_uint(t.x), by = __float_as_uint(t.y);
@@ -620,17 +613,25 @@ __global__ void __launch_bounds__(1024) k_build_tiles(BuildArgs A) {
           asm volatile("st.shared.u16 [%0], %1;" ::"r"(addr), "h"(v1));
           return v;
         };
+        // (xnew - xs0, -(ynew - ysn)) without the domain clamps: in a warp
+        // whose windows hold no edge cell a sample the clamps would move lands
+        // outside the window either way (unclamped its index is below 0 or
+        // above g-1; a NaN or a value beyond 2^22 gives bits far from
+        // 0x4B400000) and is taken again by the rescan below
         auto count_sample = [&](float2 vv) {
-          float2 xy;
+          const float2 xy = advect2(FF, csn, vv, dt2, xy1);  // move(), src/build_model.cu:284-289
           bool inw;
-          bump(vv, xy, inw);
+          bump(__ffma2_rn(xy, sgn, org), inw);
         };
-        // a warp whose windows hold edge bins: each clamp of an in-window
-        // sample outside an obstacle-overridden bin adds one r_outbound
+        // a warp whose windows hold edge bins: the domain clamps applied to the
+        // snapping coordinates (land_unit), and each clamp of a counted sample
+        // outside an obstacle-overridden bin adds one r_outbound
         auto count_sample_clamp = [&](float2 vv) {
-          float2 xy;
+          const float2 xy = advect2(FF, csn, vv, dt2, xy1);
+          const float2 d = __ffma2_rn(xy, sgn, org);
           bool inw;
-          const uint32_t v = bump(vv, xy, inw);
+          const uint32_t v =
+              bump(make_float2(fminf(fmaxf(d.x, 0.0f), axmax), fminf(fmaxf(d.y, 0.0f), aymax)), inw);
           const bool add = inw && !(v & kOvrFlag);
           n_cl += (add && (xy.x > xsn || xy.x < xs0)) ? 1 : 0;
           n_cl += (add && (xy.y > ysn || xy.y < ys0)) ? 1 : 0;
@@ -690,7 +691,10 @@ __global__ void __launch_bounds__(1024) k_build_tiles(BuildArgs A) {
       }
       if (n_out) {
         // rescan: the chunk's samples that left the window or (general loop)
-        // hit a slow bin
+        // hit a slow bin.  With unit spacing the counting loops counted exactly
+        // the samples whose clamped landing (land_unit) is in the window: the
+        // edge warps clamp, and in the others an in-window sample is never
+        // clamped
         const uint64_t m_slow = UNIT ? 0ull : masks[MASK_SLOW * nthr + tid];
         for (int q = 0; q < clen; ++q) {
           const float2 vv = myvel[q];

@@ -110,6 +110,9 @@ struct ViPack {
   int nlayers, na, na_pad, nrzns, count_type, ent_mode;
   int g, del;              // grid side and window half-width (window-offset column base)
   int gs;                  // states per group: max(1, 256 / na)
+  int na_shift;            // log2(na) when na is a power of two, else -1
+  int lps, apl;            // argmax: lanes per state (power of two), actions per lane
+  int64_t delg;            // del * (g + 1): window base(s) = s + nc - delg
   const int64_t* chunk_slot;  // nchunks + 1: first slot row of each group
   const uint16_t* maxlen;     // nchunks * 8: slot rows of each 32-row slice
   const uint8_t* perm;        // nchunks * 256: row (s_local * na + a) at each sorted position

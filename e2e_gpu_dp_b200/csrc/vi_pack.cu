@@ -142,13 +142,23 @@ __device__ __forceinline__ GroupPos group_pos(const ViPack& P, int c) {
   return r;
 }
 
-// window base of the columns of state s0 + s_local (window-offset layouts)
-__device__ __forceinline__ int64_t window_base(const ViPack& P, const GroupPos& gp, int s_local) {
-  if (gp.s0 + s_local >= P.n_row_states || gp.t + 1 >= P.nlayers) return 0;
-  const int sl = gp.sl0 + s_local;
-  const int i = sl / P.g;
-  const int j = sl - i * P.g;
-  return (int64_t)(gp.t + 1) * P.nc + (int64_t)(i - P.del) * P.g + (j - P.del);
+// Window base of the columns of state s (window-offset layouts):
+// (t+1) g^2 + (i-del) g + (j-del) = s + g^2 - del (g+1) for s = t g^2 + i g + j.
+// Only states that own rows (s < n_row_states, t+1 < nlayers) have entries.
+__device__ __forceinline__ int64_t window_base(const ViPack& P, int64_t s) {
+  if (s >= P.n_row_states) return 0;
+  return s + P.nc - P.delg;
+}
+
+// the row (s_local, a) at a sorted position from its perm byte
+__device__ __forceinline__ void row_of(const ViPack& P, int p, int& s_local, int& a) {
+  if (P.na_shift >= 0) {
+    s_local = p >> P.na_shift;
+    a = p & (P.na - 1);
+  } else {
+    s_local = p / P.na;
+    a = p - s_local * P.na;
+  }
 }
 
 // Entry streams of the three layouts:
@@ -226,9 +236,9 @@ __device__ __forceinline__ void group_q(const ViPack& P, int c, const GroupPos& 
     const int pos = (j << 5) + lane;
     if (pos >= gp.rows) continue;  // unused lanes of the group's last slice
     const int p = __ldg(P.perm + (int64_t)c * kGroupRows + pos);
-    const int s_local = p / P.na;
-    const int a = p - s_local * P.na;
-    const float* vb = MODE == ENT_I32 ? Vin : Vin + window_base(P, gp, s_local);
+    int s_local, a;
+    row_of(P, p, s_local, a);
+    const float* vb = MODE == ENT_I32 ? Vin : Vin + window_base(P, gp.s0 + s_local);
     const int64_t e0 = (slot0 + pre) * 32 + lane;
     const E cur{reinterpret_cast<const ColT*>(P.col) + e0,
                 MODE == ENT_PACKED ? nullptr : reinterpret_cast<const CntT*>(P.cnt) + e0};
@@ -254,16 +264,51 @@ __device__ __forceinline__ void group_q(const ViPack& P, int c, const GroupPos& 
   }
 }
 
-// First maximum over the actions of state s_local of a group, from q.
-__device__ __forceinline__ void state_best(const ViPack& P, const float* q, int s_local, float& bq, int& ba) {
+// First maximum over actions [a0, a1) of state s_local of a group, from q
+// (strict '>', NaN never taken: bq stays -inf / ba INT_MAX without a candidate).
+__device__ __forceinline__ void state_best(const ViPack& P, const float* q, int s_local, int a0, int a1,
+                                           float& bq, int& ba) {
   const int na1 = P.na + 1;
   bq = -INFINITY;
   ba = 0x7fffffff;
-  for (int a = 0; a < P.na; ++a) {
+  for (int a = a0; a < a1; ++a) {
     const float qa = q[s_local * na1 + a];
     if (!isnan(qa) && qa > bq) {
       bq = qa;
       ba = a;
+    }
+  }
+}
+
+// The first maximum of every state of the group, then out(s_local, bq, ba).
+// With lps > 1 lanes per state, each lane scans a block of apl actions and the
+// blocks meet by shuffles: a later block wins only with a larger value, an
+// equal value keeps the lower action -- the sequential first maximum.
+template <typename OUT>
+__device__ __forceinline__ void group_argmax(const ViPack& P, const GroupPos& gp, int lane, const float* q,
+                                             OUT&& out) {
+  const int lps = P.lps;
+  if (lps > 1) {
+    const int sl = lane >> (__ffs(lps) - 1), part = lane & (lps - 1);
+    const int a0 = min(P.na, part * P.apl), a1 = min(P.na, a0 + P.apl);
+    float bq = -INFINITY;
+    int ba = 0x7fffffff;
+    if (sl < gp.gvalid) state_best(P, q, sl, a0, a1, bq, ba);
+    for (int o = lps >> 1; o > 0; o >>= 1) {
+      const float oq = __shfl_xor_sync(kFull, bq, o);
+      const int oa = __shfl_xor_sync(kFull, ba, o);
+      if (oq > bq || (oq == bq && oa < ba)) {
+        bq = oq;
+        ba = oa;
+      }
+    }
+    if (part == 0 && sl < gp.gvalid) out(sl, bq, ba);
+  } else {
+    for (int sl = lane; sl < gp.gvalid; sl += 32) {
+      float bq;
+      int ba;
+      state_best(P, q, sl, 0, P.na, bq, ba);
+      out(sl, bq, ba);
     }
   }
 }
@@ -328,10 +373,7 @@ __global__ void __launch_bounds__(kThreads, MinBlocks<MODE, VAR>::value)
     group_q<MODE, CntT, false, Batch<VAR>::value>(P, c, gp, lane, 0, 1, Vin, q,
                                                   [&](int pos, int, int) { return ld_stream(Rg + pos); });
     __syncwarp();
-    for (int sl = lane; sl < gp.gvalid; sl += 32) {
-      float bq;
-      int ba;
-      state_best(P, q, sl, bq, ba);
+    group_argmax(P, gp, lane, q, [&](int sl, float bq, int ba) {
       float vout;
       int32_t pout;
       finish_state(bq, ba, vout, pout);
@@ -339,7 +381,7 @@ __global__ void __launch_bounds__(kThreads, MinBlocks<MODE, VAR>::value)
       if (resid) dmax = fmax(dmax, fabs((double)vout - (double)Vin[s]));
       Vout[s] = vout;
       pi[s] = pout;
-    }
+    });
     __syncwarp();  // q is rewritten by the next group
   }
   if (resid) {
@@ -416,16 +458,13 @@ __global__ void __launch_bounds__(kThreads, MinBlocks<MODE, VAR>::value)
       if (groups > 1) __syncthreads();
       else __syncwarp();
       if (active && grp == 0) {
-        for (int sl = lane; sl < gp.gvalid; sl += 32) {
-          float bq;
-          int ba;
-          state_best(P, q, sl, bq, ba);
+        group_argmax(P, gp, lane, q, [&](int sl, float bq, int ba) {
           float vout;
           int32_t pout;
           finish_state(bq, ba, vout, pout);
           V[gp.s0 + sl] = vout;
           pi[gp.s0 + sl] = pout;
-        }
+        });
       }
       if (groups > 1) __syncthreads();
       else __syncwarp();
@@ -522,11 +561,11 @@ __global__ void __launch_bounds__(kThreads, BatchMinBlocks<MODE, VAR>::value)
           const int na = P.na;
           group_q<MODE, CntT, true, Batch<VAR>::value>(
               P, c, gp, lane, grp, groups, J.V, q, [&](int pos, int s_local, int a) {
-                if (win) {
-                  const int sl = gp.sl0 + s_local;
-                  const int i = sl / P.g, jj = sl - (sl / P.g) * P.g;
+                const int sl = gp.sl0 + s_local;
+                if (win && sl >= J.wi0 * P.g && sl < (J.wi0 + J.wh) * P.g) {
+                  const int i = sl / P.g, jj = sl - i * P.g;
                   const int wi = i - J.wi0, wj = jj - J.wj0;
-                  if (wi >= 0 && wi < J.wh && wj >= 0 && wj < J.ww)
+                  if (wj >= 0 && wj < J.ww)
                     return ld_stream(J.Rwin + (((int64_t)t * J.wh + wi) * J.ww + wj) * na + a);
                 }
                 return ld_stream(Rg + pos);
@@ -540,10 +579,7 @@ __global__ void __launch_bounds__(kThreads, BatchMinBlocks<MODE, VAR>::value)
         const ViPack& P = J.P;
         if (!skip) {
           const int nc = (int)P.nc;
-          for (int sl = lane; sl < gp.gvalid; sl += 32) {
-            float bq;
-            int ba;
-            state_best(P, q, sl, bq, ba);
+          group_argmax(P, gp, lane, q, [&](int sl, float bq, int ba) {
             const int64_t s = gp.s0 + sl;
             if (J.Rwin && t + 1 < P.nlayers) {
               const int cl = gp.sl0 + sl;
@@ -565,7 +601,7 @@ __global__ void __launch_bounds__(kThreads, BatchMinBlocks<MODE, VAR>::value)
             finish_state(bq, ba, vout, po);
             J.V[s] = vout;
             J.pi[s] = po;
-          }
+          });
         }
         __syncwarp();
         if (lane == 0) {
@@ -677,16 +713,17 @@ __global__ void __launch_bounds__(kThreads) k_pack_fill(ViModel M, ViPack P, voi
     const int pos = (j << 5) + lane;
     const bool valid = pos < gp.rows;
     const int r = valid ? P.perm[(int64_t)c * kGroupRows + pos] : 0;
-    const int s_local = r / na;
+    int s_local, a;
+    row_of(P, r, s_local, a);
     const int64_t s = gp.s0 + s_local;
     const bool has = valid && s < P.n_row_states;
     int64_t rs = 0, len = 0;
     if (has) {
-      const int64_t row = s * na + (r % na);
+      const int64_t row = s * na + a;
       rs = (int64_t)rp[row];
       len = (int64_t)rp[row + 1] - rs;
     }
-    const int64_t base = MODE == ENT_I32 ? 0 : window_base(P, gp, s_local);
+    const int64_t base = MODE == ENT_I32 ? 0 : window_base(P, s);
     // padding (count 0) points at the row's own cell in layer t+1, finished
     // before layer t in every schedule, so the gathered value is finite and
     // fma(0, v, acc) leaves acc unchanged; unused lanes get the same index
@@ -798,6 +835,13 @@ cudaError_t build_pack(const ViModel& M, int64_t nc, int g, int del, PackStore* 
   P.count_type = M.count_type;
   P.g = g;
   P.del = del;
+  P.delg = (int64_t)del * (g + 1);
+  P.na_shift = -1;
+  for (int k = 0; k < 9; ++k)
+    if (P.na == (1 << k)) P.na_shift = k;
+  P.lps = 1;
+  while (P.lps * 2 * P.gs <= 32) P.lps *= 2;
+  P.apl = (P.na + P.lps - 1) / P.lps;
   const bool window =
       P.nlayers > 1 && g > 0 && (int64_t)g * g == P.nc && (int64_t)(2 * del) * (g + 1) <= 65535;
   P.ent_mode = !window ? ENT_I32 : (M.count_type == CNT_U16 ? ENT_PACKED : ENT_OFF16);

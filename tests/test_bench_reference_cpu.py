@@ -75,3 +75,24 @@ def test_vi_bytes_and_issue_roofline():
     r = bench.k1_issue_roofline(samples=32 * 10**9, k1_s=1.0, sm_mhz=1000.0, n_sm=100)
     assert r is not None and r["peak"] == 100 * 4 * 1e9
     assert abs(r["achieved"] - r["warp_inst_per_sample"] * 32e9) < 1e-3
+
+
+def test_parity_sample_counts_each_row_once():
+    """A row one entry longer on the device is one mismatched row; the rows
+    after it still compare equal."""
+    import numpy as np
+
+    from oracle import pyoracle as O
+    from tests.helpers import problem
+
+    prob, fields = problem("t_time")
+    full = O.build_model(prob, fields, nthreads=2)
+    r0 = 1000
+    blk = O.build_rows(prob, fields, r0=r0, r1=r0 + 200, nthreads=2)
+    rp = full["row_ptr"].copy()
+    k = int(rp[r0 + 10])
+    col = np.insert(full["col"].astype(np.int32), k, 7)
+    cnt = np.insert(full["cnt"], k, 1)
+    rp[r0 + 11:] += 1
+    h = {"row_ptr": rp, "col": col, "cnt": cnt, "R": full["R_full"]}
+    assert bench.parity_sample(h, [(r0, blk)])["mismatched_rows"] == 1
