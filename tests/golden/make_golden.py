@@ -36,7 +36,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, ROOT)
 
-NAMES = ["t_time", "t_custom", "t_energy2", "t_wide", "c1"]
+NAMES = ["t_time", "t_custom", "t_energy2", "t_wide", "c1", "t_m10", "t_m8", "t_m6", "t_energy1", "t_energy3",
+         "t_half"]
 
 
 def fields_digest(fields) -> str:

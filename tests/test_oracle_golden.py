@@ -14,7 +14,7 @@ from oracle import pyoracle as O
 from tests.golden.make_golden import NAMES, decode, fields_digest
 from tests.helpers import VALUE_RTOL, golden, policy_ok, problem, q_values_f64, values_close
 
-INTEGER_REWARDS = {"t_time", "t_wide", "c1"}
+from tests.helpers import INTEGER_REWARDS  # noqa: E402
 NTHREADS = max(1, min(8, os.cpu_count() or 1))
 
 
