@@ -210,14 +210,15 @@ __device__ __forceinline__ void decode(ColT o, CntT w, uint32_t& idx, float& f) 
 }
 
 // Q of the rows of this warp's slices of group c (slices j0, j0 + jstep, ...)
-// into q[s_local * (na + 1) + a]: the row's FMA chain in entry order, B
-// entries loaded before their gathers, then finish_row with R = rfun(sorted
-// position, s_local, a).
+// into q[s_local * (na + 1) + a]: the row's FMA chain in entry order, then
+// finish_row with R = rfun(sorted position, s_local, a).  Entries come B at a
+// time without branches: positions at or beyond the slice's maxlen reload
+// the slice's last entry of the row (an L1 hit) with weight 0, and
+// fma(0, v, acc) == acc for the finite v it points at.
 template <int MODE, typename CntT, bool COHERENT, int B, typename RF>
 __device__ __forceinline__ void group_q(const ViPack& P, int c, const GroupPos& gp, int lane, int j0,
                                         int jstep, const float* Vin, float* q, RF&& rfun) {
-  using E = Entries<MODE, CntT>;
-  using ColT = typename E::ColT;
+  using ColT = typename Entries<MODE, CntT>::ColT;
   const int nsl = (gp.rows + 31) >> 5;
   // slot rows of the slices (lane j: slice j) and their inclusive prefix
   const int mlj = lane < kSlices ? (int)__ldg(P.maxlen + (int64_t)c * kSlices + lane) : 0;
@@ -227,40 +228,57 @@ __device__ __forceinline__ void group_q(const ViPack& P, int c, const GroupPos& 
     const int t2 = __shfl_up_sync(kFull, incl, o);
     if (lane >= o) incl += t2;
   }
-  const int64_t slot0 = __ldg(P.chunk_slot + c);
+  // everything the slice loop needs, in registers
+  const int64_t e0 = __ldg(P.chunk_slot + c) * 32 + lane;
+  const ColT* colg = reinterpret_cast<const ColT*>(P.col) + e0;
+  const CntT* cntg = MODE == ENT_PACKED ? nullptr : reinterpret_cast<const CntT*>(P.cnt) + e0;
+  const uint8_t* permg = P.perm + (int64_t)c * kGroupRows + lane;
+  const int na = P.na, na1 = na + 1, na_shift = P.na_shift;
+  const int64_t nrs = P.n_row_states, woff = P.nc - P.delg;
   const bool counts = P.count_type != VAL_F32;
-  const int na1 = P.na + 1;
+  const float fn = (float)P.nrzns;
   for (int j = j0; j < nsl; j += jstep) {
     const int ml = __shfl_sync(kFull, mlj, j);
     const int pre = __shfl_sync(kFull, incl, j) - ml;
     const int pos = (j << 5) + lane;
     if (pos >= gp.rows) continue;  // unused lanes of the group's last slice
-    const int p = __ldg(P.perm + (int64_t)c * kGroupRows + pos);
+    const int p = __ldg(permg + (j << 5));
     int s_local, a;
-    row_of(P, p, s_local, a);
-    const float* vb = MODE == ENT_I32 ? Vin : Vin + window_base(P, gp.s0 + s_local);
-    const int64_t e0 = (slot0 + pre) * 32 + lane;
-    const E cur{reinterpret_cast<const ColT*>(P.col) + e0,
-                MODE == ENT_PACKED ? nullptr : reinterpret_cast<const CntT*>(P.cnt) + e0};
+    if (na_shift >= 0) {
+      s_local = p >> na_shift;
+      a = p & (na - 1);
+    } else {
+      s_local = p / na;
+      a = p - s_local * na;
+    }
+    const int64_t s = gp.s0 + s_local;
+    // window base of the row's columns: s + g^2 - del (g+1) (rows exist only for s < n_row_states)
+    const float* vb = MODE == ENT_I32 ? Vin : Vin + (s < nrs ? s + woff : 0);
+    const ColT* ce = colg + (pre << 5);
+    const CntT* cw = MODE == ENT_PACKED ? nullptr : cntg + (pre << 5);
     const float r = rfun(pos, s_local, a);
     float acc = 0.f;
     for (int k0 = 0; k0 < ml; k0 += B) {
-      const int n = min(ml - k0, B);
       ColT o[B];
       CntT w[B];
-      cur.template load<B>(k0, n, o, w);
+#pragma unroll
+      for (int jj = 0; jj < B; ++jj) {
+        const int k = min(k0 + jj, ml - 1);
+        o[jj] = ld_stream(ce + (k << 5));
+        w[jj] = MODE != ENT_PACKED ? ld_stream(cw + (k << 5)) : (CntT)0;
+      }
       float v[B], f[B];
 #pragma unroll
       for (int jj = 0; jj < B; ++jj) {
         uint32_t idx;
         decode<MODE, ColT, CntT>(o[jj], w[jj], idx, f[jj]);
-        v[jj] = jj < n ? ld_value<COHERENT>(vb + idx) : 0.f;
+        if (k0 + jj >= ml) f[jj] = 0.f;
+        v[jj] = ld_value<COHERENT>(vb + idx);
       }
-      // entries beyond n hold count 0 and v = 0: fma(0, 0, acc) == acc
 #pragma unroll
       for (int jj = 0; jj < B; ++jj) acc = fmaf(f[jj], v[jj], acc);
     }
-    q[s_local * na1 + a] = finish_row(r, acc, 0.f, P.nrzns, counts);
+    q[s_local * na1 + a] = counts ? r + acc / fn : r + acc;  // finish_row
   }
 }
 
