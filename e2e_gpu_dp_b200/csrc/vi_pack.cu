@@ -53,7 +53,7 @@ constexpr int kThreads = 256;
 constexpr int kWarps = kThreads / 32;
 constexpr int kSlices = 8;          // slices of 32 rows per group
 constexpr int kGroupRows = 256;     // rows per group (G * na <= 256)
-constexpr int kQStride = 512;       // shared Q floats per group: G * (na + 1) <= 512
+constexpr int kQStride = 512;       // shared Q floats per group: G * (na + 1) <= 512, plus a spare
 constexpr int kLenKeys = 64;        // sort keys: row lengths 0..63, longer rows as 63
 constexpr int PF_NEXT = VI_TUNE_PF_NEXT;
 constexpr int PF_CURRENT = VI_TUNE_PF_CURRENT;
@@ -241,7 +241,9 @@ __device__ __forceinline__ void group_q(const ViPack& P, int c, const GroupPos& 
     const int ml = __shfl_sync(kFull, mlj, j);
     const int pre = __shfl_sync(kFull, incl, j) - ml;
     const int pos = (j << 5) + lane;
-    if (pos >= gp.rows) continue;  // unused lanes of the group's last slice
+    // unused lanes of a partial group's last slice read the padding the pack
+    // holds for them (perm 0, count 0, R 0) and write a spare slot of q
+    const bool used = pos < gp.rows;
     const int p = __ldg(permg + (j << 5));
     int s_local, a;
     if (na_shift >= 0) {
@@ -278,7 +280,7 @@ __device__ __forceinline__ void group_q(const ViPack& P, int c, const GroupPos& 
 #pragma unroll
       for (int jj = 0; jj < B; ++jj) acc = fmaf(f[jj], v[jj], acc);
     }
-    q[s_local * na1 + a] = counts ? r + acc / fn : r + acc;  // finish_row
+    q[used ? s_local * na1 + a : kQStride] = counts ? r + acc / fn : r + acc;  // finish_row
   }
 }
 
@@ -377,7 +379,7 @@ template <int MODE, typename CntT, int VAR>
 __global__ void __launch_bounds__(kThreads, MinBlocks<MODE, VAR>::value)
     k_vi_chunks(ViPack P, int c_begin, int c_end, const float* __restrict__ Vin, float* Vout, int32_t* pi,
                 unsigned long long* resid, int prefetch) {
-  __shared__ float qs[kWarps][kQStride];
+  __shared__ float qs[kWarps][kQStride + 1];
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   const int nw = gridDim.x * kWarps;
   float* q = qs[wid];
@@ -452,7 +454,7 @@ __device__ __forceinline__ bool grid_barrier(unsigned int* sync, unsigned int ta
 template <int MODE, typename CntT, int VAR>
 __global__ void __launch_bounds__(kThreads, MinBlocks<MODE, VAR>::value)
     k_vi_layered(ViPack P, int groups, float* V, int32_t* pi, unsigned int* sync, int prefetch, WaitBound wb) {
-  __shared__ float qs[kWarps][kQStride];
+  __shared__ float qs[kWarps][kQStride + 1];
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   const int cpc = kWarps / groups;  // groups of states per CTA iteration
   const int grp = wid % groups, slot_in_cta = wid / groups;
@@ -517,7 +519,7 @@ template <int MODE, typename CntT, int VAR>
 __global__ void __launch_bounds__(kThreads, BatchMinBlocks<MODE, VAR>::value)
     k_vi_batch(const unsigned char* table, int job_cap, int groups, int* done, int layer_cap,
                unsigned int* err, int prefetch, WaitBound wb) {
-  __shared__ float qs[kWarps][kQStride];
+  __shared__ float qs[kWarps][kQStride + 1];
   const ViBatchHeader* H = reinterpret_cast<const ViBatchHeader*>(table);
   const ViJob* jobs = reinterpret_cast<const ViJob*>(table + kViBatchJobsOffset);
   const int* cum = reinterpret_cast<const int*>(jobs + job_cap);
@@ -680,10 +682,14 @@ __global__ void __launch_bounds__(kThreads) k_pack_count(ViModel M, ViPack P, in
     off[wid][2 * lane + 1] = ex + v0;
   }
   __syncwarp();
-  // stable placement, 32 rows at a time in row order
+  // stable placement, 32 rows at a time, rows of equal length in
+  // action-major order (u = a * gvalid + s_local): a slice then holds few
+  // actions over consecutive states, whose V gathers share cache lines
   for (int base = 0; base < gp.rows; base += 32) {
-    const int r = base + lane;
-    const bool has = r < gp.rows;
+    const int u = base + lane;
+    const bool has = u < gp.rows;
+    const int ua = has ? u / gp.gvalid : 0;
+    const int r = has ? (u - ua * gp.gvalid) * na + ua : 0;
     const int key = has ? key_of(lens[wid][r]) : kLenKeys + lane;
     const unsigned m = __match_any_sync(kFull, key);
     const int rank = __popc(m & ((1u << lane) - 1u));
