@@ -104,26 +104,21 @@ enum : int {
 
 struct ViPack {
   int64_t ns, nc;          // states; states per layer (ns when the model has no layers)
-  int64_t cpl, nchunks;    // groups of gs states per layer; all groups
+  int64_t cpl, nchunks;    // chunks of 32 states per layer; all chunks
   int64_t n_row_states;    // states that own rows
   int64_t slot_rows;       // slot rows of 32 entries
   int nlayers, na, na_pad, nrzns, count_type, ent_mode;
   int g, del;              // grid side and window half-width (window-offset column base)
-  int gs;                  // states per group: max(1, 256 / na)
-  int na_shift;            // log2(na) when na is a power of two, else -1
-  int lps, apl;            // argmax: lanes per state (power of two), actions per lane
-  int64_t delg;            // del * (g + 1): window base(s) = s + nc - delg
-  const int64_t* chunk_slot;  // nchunks + 1: first slot row of each group
-  const uint16_t* maxlen;     // nchunks * 8: slot rows of each 32-row slice
-  const uint8_t* perm;        // nchunks * 256: row (s_local * na + a) at each sorted position
+  const int64_t* chunk_slot;  // nchunks + 1: first slot row of each chunk
+  const uint16_t* maxlen;     // nchunks * na_pad: slot rows per (chunk, action)
   const void* col;            // slot_rows * 32: packed entries, uint16 offsets or int32 columns
   const void* cnt;            // slot_rows * 32: counts / values (null for ENT_PACKED)
-  const float* R;             // nchunks * 256: R at each sorted position
+  const float* R;             // nchunks * na * 32: [chunk][action][lane]
 };
 
 struct PackStore {
   ViPack v{};
-  void* bufs[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
+  void* bufs[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
   int64_t bytes = 0;
 };
 
@@ -134,19 +129,19 @@ cudaError_t build_pack(const ViModel& M, int64_t nc, int g, int del, PackStore* 
 void free_pack(PackStore* p);
 // bytes one sweep over the pack moves (entries with padding, R, tables, V)
 int64_t pack_sweep_bytes(const ViPack& P);
-// tune bits of the sweeps: L2 bulk prefetch of the group a warp takes next
-// (the next layer's, when layered) and/or of the group it starts; the lean
-// kernel (4 entries a batch, 8 CTAs per SM) instead of the 8-entry one (5
-// CTAs per SM).  Bit 3 is accepted and has no effect.
-enum : int { VI_TUNE_PF_NEXT = 1, VI_TUNE_PF_CURRENT = 2, VI_TUNE_LEAN = 4 };
-// One Jacobi sweep over groups [c_begin, c_end).
-// err: unused (kept for callers that pass their error word)
+// tune bits of the sweeps: L2 bulk prefetch of the chunk a warp takes next
+// (the next layer's, when layered) and/or of the chunk it starts; the lean
+// kernel (no entry look-ahead, 8 CTAs per SM) instead of the look-ahead one;
+// for the Jacobi sweep of the packed layout, the TMA-staged kernel
+enum : int { VI_TUNE_PF_NEXT = 1, VI_TUNE_PF_CURRENT = 2, VI_TUNE_LEAN = 4, VI_TUNE_TMA = 8 };
+// One Jacobi sweep over chunks [c_begin, c_end).
+// err: device word for bounded-wait failures (needed by the TMA-staged kernel)
 cudaError_t launch_vi_chunks(const ViPack& P, int64_t c_begin, int64_t c_end, const float* Vin,
                              float* Vout, int32_t* pi, unsigned long long* resid, cudaStream_t st,
                              int tune, unsigned int* err = nullptr);
 // The whole layered schedule in one cooperative launch, in place on V.
-// sync: two zeroed words (barrier count, error bits); groups: warps per group
-// of states (1, 2, 4, 8; 0 picks one).
+// sync: two zeroed words (barrier count, error bits); groups: warps per chunk
+// (1, 2, 4, 8; 0 picks one).
 cudaError_t launch_vi_layered(const ViPack& P, float* V, int32_t* pi, unsigned int* sync, int groups,
                               cudaStream_t st, int tune);
 
@@ -167,9 +162,9 @@ struct ViBatchHeader {
   int njobs, max_layers, pad0, pad1;
 };
 // Device table: header | jobs[job_cap] | cum[job_cap + 1] | nact[layer_cap].
-// Jobs sorted by nlayers, descending; cum = prefix sums of their groups per
+// Jobs sorted by nlayers, descending; cum = prefix sums of their chunks per
 // layer; nact[k] = jobs with more than k layers.  Step k of the launch works
-// on layer nlayers-1-k of jobs [0, nact[k]): group items [0, cum[nact[k]]),
+// on layer nlayers-1-k of jobs [0, nact[k]): chunk items [0, cum[nact[k]]),
 // each waiting only for its own job's next layer.
 size_t vi_batch_table_bytes(int job_cap, int layer_cap);
 constexpr size_t kViBatchJobsOffset = 64;  // header padded to 64 bytes

@@ -1,20 +1,14 @@
 // K5 + K6: the sliced copy of a model that value iteration streams, and the
 // sweeps over it.
 //
-// Layout: row-sorted groups.  States are taken in groups of G = max(1, 256/na)
-// consecutive states of one layer (a group never crosses a layer boundary;
-// the last group of a layer may be partial), i.e. at most 256 rows (s, a).
-// Within a group the rows are ordered by length, longest first (stable in row
-// order; lengths above 63 count as 63), and cut into slices of 32: lane l of
-// slice j holds the row at sorted position 32j + l.  Slice j stores
-// maxlen[group][j] slot rows of 32 entries, so entry k of the slice's 32 rows
-// is one coalesced line:
-//   slot (chunk_slot[group] + sum_{i<j} maxlen[group][i] + k) * 32 + l.
-// Rows shorter than their slice's maxlen are padded with count 0.  Sorting
-// keeps rows of similar length in a slice: on the 200x200x120 model the
-// padding is 7 % of the entries (33.7 % with one row per lane for 32 states of
-// one action).  Per sorted position the group stores the row (perm, one byte:
-// s_local * na + a) and its R.
+// Layout.  States are taken in chunks of 32 consecutive states of one layer
+// (a chunk never crosses a layer boundary; the last chunk of a layer is
+// partial).  Lane l of a warp owns state l of a chunk.  For action a, a chunk
+// stores maxlen[c][a] "slot rows" of 32 entries; entry k of row (s, a) sits at
+//   slot (chunk_slot[c] + sum_{b<a} maxlen[c][b] + k) * 32 + lane(s)
+// so the k-th entries of the 32 rows (s, a) of a chunk are one coalesced
+// 128-byte line.  Rows shorter than maxlen are padded with count 0.  R is
+// stored beside it as [chunk][action][lane].
 //
 // Columns: on a time-layered model built on a g x g grid, every next state of
 // a layer-t cell (i, j) lies in layer t+1 inside the m x m window centred on
@@ -27,16 +21,15 @@
 // other solver path of this package (finish_row), followed by fma(0, v, acc)
 // for each padding slot, which returns acc unchanged as long as v is finite
 // (acc is never -0: it starts at +0 and RN addition gives -0 only from two -0
-// operands).  A padding slot therefore points at the row's own cell in layer
+// operands).  A padding slot therefore points at the lane's own cell in layer
 // t+1, whose value is final before layer t is computed in any schedule, never
-// at memory the current sweep has not written yet.  The rows' Q values go to
-// shared memory at (s_local, a); the first-maximum argmax then runs per state
-// in action order (the reference's select_best_action, src/spvi_2.cu:93-122:
-// start -1e6 / -1, strict '>', NaN never taken).  Values are bit-identical to
-// the CSR sweep.
+// at memory the current sweep has not written yet.  Values are bit-identical
+// to the CSR sweep.
 //
-// Per row the sweep reads (offset + count) per padded entry, R, one perm byte
-// and the gathered V; there is no row pointer.
+// Per row the sweep reads (offset + count) per padded entry, R, and the
+// gathered V; there is no row pointer.  The first-maximum argmax is taken
+// in action order inside the lane (the reference's select_best_action,
+// src/spvi_2.cu:93-122: start -1e6 / -1, strict '>').
 #include <math.h>
 
 #include <algorithm>
@@ -51,15 +44,10 @@ namespace {
 
 constexpr int kThreads = 256;
 constexpr int kWarps = kThreads / 32;
-constexpr int kSlices = 8;          // slices of 32 rows per group
-constexpr int kGroupRows = 256;     // rows per group (G * na <= 256)
-constexpr int kQStride = 512;       // shared Q floats per group: G * (na + 1) <= 512, plus a spare
-constexpr int kLenKeys = 64;        // sort keys: row lengths 0..63, longer rows as 63
 constexpr int PF_NEXT = VI_TUNE_PF_NEXT;
 constexpr int PF_CURRENT = VI_TUNE_PF_CURRENT;
 constexpr long long kBarrierSpinLimit = 1ll << 22;
 constexpr unsigned long long kBarrierTimeoutNs = 2000000000ull;  // 2 s
-constexpr unsigned kFull = 0xffffffffu;
 
 // Bounds of the device-side waits of the persistent sweeps (grid barriers of
 // the layered sweep, per-layer completion counters of the batched sweep): a
@@ -124,41 +112,27 @@ __device__ __forceinline__ float ld_value(const float* p) {
   return __ldg(p);
 }
 
-// Position of group c: first state, layer, its index in the layer, states and rows.
-struct GroupPos {
-  int64_t s0;
-  int t, sl0, gvalid, rows;
+struct ChunkPos {
+  int64_t s;      // state of this lane
+  int64_t base;   // window base of the lane's columns (window-offset layouts) or 0
+  bool valid;     // the lane's state exists
 };
 
-// group indices, layer sizes and grid sides fit in 32 bits (checked on the host)
-__device__ __forceinline__ GroupPos group_pos(const ViPack& P, int c) {
-  GroupPos r;
+// chunk indices, layer sizes and grid sides fit in 32 bits (checked on the host)
+__device__ __forceinline__ ChunkPos chunk_pos(const ViPack& P, int c, int lane, bool window) {
+  ChunkPos r;
   const int cpl = (int)P.cpl, nc = (int)P.nc;
-  r.t = c / cpl;
-  r.sl0 = (c - r.t * cpl) * P.gs;
-  r.gvalid = min(P.gs, nc - r.sl0);
-  r.s0 = (int64_t)r.t * nc + r.sl0;
-  r.rows = r.gvalid * P.na;
-  return r;
-}
-
-// Window base of the columns of state s (window-offset layouts):
-// (t+1) g^2 + (i-del) g + (j-del) = s + g^2 - del (g+1) for s = t g^2 + i g + j.
-// Only states that own rows (s < n_row_states, t+1 < nlayers) have entries.
-__device__ __forceinline__ int64_t window_base(const ViPack& P, int64_t s) {
-  if (s >= P.n_row_states) return 0;
-  return s + P.nc - P.delg;
-}
-
-// the row (s_local, a) at a sorted position from its perm byte
-__device__ __forceinline__ void row_of(const ViPack& P, int p, int& s_local, int& a) {
-  if (P.na_shift >= 0) {
-    s_local = p >> P.na_shift;
-    a = p & (P.na - 1);
-  } else {
-    s_local = p / P.na;
-    a = p - s_local * P.na;
+  const int t = c / cpl;
+  const int sl = (c - t * cpl) * 32 + lane;
+  r.valid = sl < nc;
+  r.s = (int64_t)t * nc + sl;
+  r.base = 0;
+  if (window && r.valid && r.s < P.n_row_states && t + 1 < P.nlayers) {
+    const int i = sl / P.g;
+    const int j = sl - i * P.g;
+    r.base = (int64_t)(t + 1) * nc + (int64_t)(i - P.del) * P.g + (j - P.del);
   }
+  return r;
 }
 
 // Entry streams of the three layouts:
@@ -172,16 +146,18 @@ struct Entries {
       typename std::conditional<MODE == ENT_OFF16, uint16_t, int32_t>::type>::type;
   const ColT* col;
   const CntT* cnt;
-  // entries k0 .. k0+n-1 (n <= B) of this lane's row, zeros beyond
+  __device__ __forceinline__ void advance(int rows) {
+    col += rows * 32;
+    if (MODE != ENT_PACKED) cnt += rows * 32;
+  }
+  // this lane's first n (<= B) entries, zeros beyond; a full batch loads unpredicated
   template <int B>
-  __device__ __forceinline__ void load(int k0, int n, ColT (&o)[B], CntT (&w)[B]) const {
-    const ColT* cp = col + (int64_t)k0 * 32;
-    const CntT* wp = MODE != ENT_PACKED ? cnt + (int64_t)k0 * 32 : nullptr;
+  __device__ __forceinline__ void load(int n, ColT (&o)[B], CntT (&w)[B]) const {
     if (n == B) {
 #pragma unroll
       for (int j = 0; j < B; ++j) {
-        o[j] = ld_stream(cp + j * 32);
-        w[j] = MODE != ENT_PACKED ? ld_stream(wp + j * 32) : (CntT)0;
+        o[j] = ld_stream(col + j * 32);
+        w[j] = MODE != ENT_PACKED ? ld_stream(cnt + j * 32) : (CntT)0;
       }
       return;
     }
@@ -190,8 +166,8 @@ struct Entries {
       o[j] = 0;
       w[j] = 0;
       if (j < n) {
-        o[j] = ld_stream(cp + j * 32);
-        if (MODE != ENT_PACKED) w[j] = ld_stream(wp + j * 32);
+        o[j] = ld_stream(col + j * 32);
+        if (MODE != ENT_PACKED) w[j] = ld_stream(cnt + j * 32);
       }
     }
   }
@@ -209,128 +185,108 @@ __device__ __forceinline__ void decode(ColT o, CntT w, uint32_t& idx, float& f) 
   }
 }
 
-// Q of the rows of this warp's slices of group c (slices j0, j0 + jstep, ...)
-// into q[s_local * (na + 1) + a]: the row's FMA chain in entry order, then
-// finish_row with R = rfun(sorted position, s_local, a).  Entries come B at a
-// time without branches: positions at or beyond the slice's maxlen reload
-// the slice's last entry of the row (an L1 hit) with weight 0, and
-// fma(0, v, acc) == acc for the finite v it points at.
-template <int MODE, typename CntT, bool COHERENT, int B, typename RF>
-__device__ __forceinline__ void group_q(const ViPack& P, int c, const GroupPos& gp, int lane, int j0,
-                                        int jstep, const float* Vin, float* q, RF&& rfun) {
-  using ColT = typename Entries<MODE, CntT>::ColT;
-  const int nsl = (gp.rows + 31) >> 5;
-  // slot rows of the slices (lane j: slice j) and their inclusive prefix
-  const int mlj = lane < kSlices ? (int)__ldg(P.maxlen + (int64_t)c * kSlices + lane) : 0;
-  int incl = mlj;
-#pragma unroll
-  for (int o = 1; o < kSlices; o <<= 1) {
-    const int t2 = __shfl_up_sync(kFull, incl, o);
-    if (lane >= o) incl += t2;
-  }
-  // everything the slice loop needs, in registers
-  const int64_t e0 = __ldg(P.chunk_slot + c) * 32 + lane;
-  const ColT* colg = reinterpret_cast<const ColT*>(P.col) + e0;
-  const CntT* cntg = MODE == ENT_PACKED ? nullptr : reinterpret_cast<const CntT*>(P.cnt) + e0;
-  const uint8_t* permg = P.perm + (int64_t)c * kGroupRows + lane;
-  const int na = P.na, na1 = na + 1, na_shift = P.na_shift;
-  const int64_t nrs = P.n_row_states, woff = P.nc - P.delg;
+// Best (value, action) over actions [a0, a1) of the lane's state of chunk c;
+// the lane's R of action a is Rp[(a - a0) * rstride].  VAR 0: the next
+// action's first batch of 4 entries is loaded before this action's gathers
+// (5 CTAs per SM).  VAR 1: no look-ahead, fewer registers and 8 CTAs per SM;
+// latency is hidden by the extra warps instead.
+template <int MODE, typename CntT, bool COHERENT, int VAR>
+__device__ __forceinline__ void chunk_best(const ViPack& P, int c, const ChunkPos& cp, int lane, int a0,
+                                           int a1, const float* Vin, float& bq, int& ba,
+                                           const float* Rp, int rstride) {
+  using E = Entries<MODE, CntT>;
+  using ColT = typename E::ColT;
+  constexpr int B = 4;
+  const uint16_t* mlp = P.maxlen + (int64_t)c * P.na_pad;
+  int64_t slot = __ldg(P.chunk_slot + c);
+  for (int b = 0; b < a0; ++b) slot += __ldg(mlp + b);
+  E cur{reinterpret_cast<const ColT*>(P.col) + slot * 32 + lane,
+        MODE == ENT_PACKED ? nullptr : reinterpret_cast<const CntT*>(P.cnt) + slot * 32 + lane};
+  const float* vb = MODE == ENT_I32 ? Vin : Vin + cp.base;
   const bool counts = P.count_type != VAL_F32;
-  const float fn = (float)P.nrzns;
-  for (int j = j0; j < nsl; j += jstep) {
-    const int ml = __shfl_sync(kFull, mlj, j);
-    const int pre = __shfl_sync(kFull, incl, j) - ml;
-    const int pos = (j << 5) + lane;
-    // unused lanes of a partial group's last slice read the padding the pack
-    // holds for them (perm 0, count 0, R 0) and write a spare slot of q
-    const bool used = pos < gp.rows;
-    const int p = __ldg(permg + (j << 5));
-    int s_local, a;
-    if (na_shift >= 0) {
-      s_local = p >> na_shift;
-      a = p & (na - 1);
-    } else {
-      s_local = p / na;
-      a = p - s_local * na;
+  auto fold = [&](const ColT(&o)[B], const CntT(&w)[B], int n, float& acc) {
+    float v[B], f[B];
+#pragma unroll
+    for (int j = 0; j < B; ++j) {
+      uint32_t idx;
+      decode<MODE, ColT, CntT>(o[j], w[j], idx, f[j]);
+      v[j] = j < n ? ld_value<COHERENT>(vb + idx) : 0.f;
     }
-    const int64_t s = gp.s0 + s_local;
-    // window base of the row's columns: s + g^2 - del (g+1) (rows exist only for s < n_row_states)
-    const float* vb = MODE == ENT_I32 ? Vin : Vin + (s < nrs ? s + woff : 0);
-    const ColT* ce = colg + (pre << 5);
-    const CntT* cw = MODE == ENT_PACKED ? nullptr : cntg + (pre << 5);
-    const float r = rfun(pos, s_local, a);
-    float acc = 0.f;
-    for (int k0 = 0; k0 < ml; k0 += B) {
-      ColT o[B];
-      CntT w[B];
+    // entries beyond n hold count 0 and v = 0: fma(0, 0, acc) == acc
 #pragma unroll
-      for (int jj = 0; jj < B; ++jj) {
-        const int k = min(k0 + jj, ml - 1);
-        o[jj] = ld_stream(ce + (k << 5));
-        w[jj] = MODE != ENT_PACKED ? ld_stream(cw + (k << 5)) : (CntT)0;
-      }
-      float v[B], f[B];
-#pragma unroll
-      for (int jj = 0; jj < B; ++jj) {
-        uint32_t idx;
-        decode<MODE, ColT, CntT>(o[jj], w[jj], idx, f[jj]);
-        if (k0 + jj >= ml) f[jj] = 0.f;
-        v[jj] = ld_value<COHERENT>(vb + idx);
-      }
-#pragma unroll
-      for (int jj = 0; jj < B; ++jj) acc = fmaf(f[jj], v[jj], acc);
-    }
-    q[used ? s_local * na1 + a : kQStride] = counts ? r + acc / fn : r + acc;  // finish_row
-  }
-}
-
-// First maximum over actions [a0, a1) of state s_local of a group, from q
-// (strict '>', NaN never taken: bq stays -inf / ba INT_MAX without a candidate).
-__device__ __forceinline__ void state_best(const ViPack& P, const float* q, int s_local, int a0, int a1,
-                                           float& bq, int& ba) {
-  const int na1 = P.na + 1;
-  bq = -INFINITY;
-  ba = 0x7fffffff;
+    for (int j = 0; j < B; ++j) acc = fmaf(f[j], v[j], acc);
+  };
+  int ml = a0 < a1 ? __ldg(mlp + a0) : 0;
+  ColT o[B];
+  CntT w[B];
+  if (VAR == 0) cur.template load<B>(min(ml, B), o, w);
   for (int a = a0; a < a1; ++a) {
-    const float qa = q[s_local * na1 + a];
-    if (!isnan(qa) && qa > bq) {
-      bq = qa;
+    const float r = ld_stream(Rp);
+    Rp += rstride;
+    float acc = 0.f;
+    int mln = 0;
+    E nxt = cur;
+    nxt.advance(ml);
+    if (VAR == 0) {
+      mln = a + 1 < a1 ? __ldg(mlp + a + 1) : 0;
+      ColT no[B];
+      CntT nw[B];
+      nxt.template load<B>(min(mln, B), no, nw);
+      fold(o, w, min(ml, B), acc);
+#pragma unroll
+      for (int j = 0; j < B; ++j) {
+        o[j] = no[j];
+        w[j] = nw[j];
+      }
+    } else {
+      cur.template load<B>(min(ml, B), o, w);
+      fold(o, w, min(ml, B), acc);
+    }
+    for (int k0 = B; k0 < ml; k0 += B) {  // rows longer than one batch
+      E more = cur;
+      more.advance(k0);
+      ColT o2[B];
+      CntT w2[B];
+      more.template load<B>(min(ml - k0, B), o2, w2);
+      fold(o2, w2, min(ml - k0, B), acc);
+    }
+    const float q = finish_row(r, acc, 0.f, P.nrzns, counts);
+    if (!isnan(q) && q > bq) {
+      bq = q;
       ba = a;
     }
+    cur = nxt;
+    if (VAR == 0) ml = mln;
+    else ml = a + 1 < a1 ? __ldg(mlp + a + 1) : 0;
   }
 }
 
-// The first maximum of every state of the group, then out(s_local, bq, ba).
-// With lps > 1 lanes per state, each lane scans a block of apl actions and the
-// blocks meet by shuffles: a later block wins only with a larger value, an
-// equal value keeps the lower action -- the sequential first maximum.
-template <typename OUT>
-__device__ __forceinline__ void group_argmax(const ViPack& P, const GroupPos& gp, int lane, const float* q,
-                                             OUT&& out) {
-  const int lps = P.lps;
-  if (lps > 1) {
-    const int sl = lane >> (__ffs(lps) - 1), part = lane & (lps - 1);
-    const int a0 = min(P.na, part * P.apl), a1 = min(P.na, a0 + P.apl);
-    float bq = -INFINITY;
-    int ba = 0x7fffffff;
-    if (sl < gp.gvalid) state_best(P, q, sl, a0, a1, bq, ba);
-    for (int o = lps >> 1; o > 0; o >>= 1) {
-      const float oq = __shfl_xor_sync(kFull, bq, o);
-      const int oa = __shfl_xor_sync(kFull, ba, o);
-      if (oq > bq || (oq == bq && oa < ba)) {
-        bq = oq;
-        ba = oa;
-      }
-    }
-    if (part == 0 && sl < gp.gvalid) out(sl, bq, ba);
-  } else {
-    for (int sl = lane; sl < gp.gvalid; sl += 32) {
-      float bq;
-      int ba;
-      state_best(P, q, sl, 0, P.na, bq, ba);
-      out(sl, bq, ba);
-    }
+// R of (lane's state, action a0) in the pack's [chunk][action][lane] table
+__device__ __forceinline__ const float* pack_r(const ViPack& P, int c, int a0, int lane) {
+  return P.R + ((int64_t)c * P.na + a0) * 32 + lane;
+}
+
+template <int MODE, int VAR>
+struct MinBlocks {
+  static constexpr int value = MODE != ENT_PACKED ? 3 : (VAR == 0 ? 5 : 8);
+};
+
+template <int MODE, typename CntT>
+struct Widths {
+  static constexpr int col = MODE == ENT_OFF16 ? 2 : 4;
+  static constexpr int cnt = MODE == ENT_PACKED ? 0 : (int)sizeof(CntT);
+};
+
+// L2 prefetch of chunk c: entry streams and R (bulk prefetch, one lane)
+__device__ __forceinline__ void prefetch_chunk(const ViPack& P, int c, int col_bytes, int cnt_bytes) {
+  const int64_t s0 = __ldg(P.chunk_slot + c), s1 = __ldg(P.chunk_slot + c + 1);
+  const int64_t n = (s1 - s0) * 32;
+  if (n > 0) {
+    prefetch_l2(reinterpret_cast<const char*>(P.col) + s0 * 32 * col_bytes, (uint32_t)(n * col_bytes));
+    if (cnt_bytes)
+      prefetch_l2(reinterpret_cast<const char*>(P.cnt) + s0 * 32 * cnt_bytes, (uint32_t)(n * cnt_bytes));
   }
+  prefetch_l2(P.R + (int64_t)c * P.na * 32, (uint32_t)(P.na * 32 * 4));
 }
 
 __device__ __forceinline__ void finish_state(float bq, int ba, float& vout, int32_t& pout) {
@@ -343,73 +299,248 @@ __device__ __forceinline__ void finish_state(float bq, int ba, float& vout, int3
   }
 }
 
-template <int MODE, typename CntT>
-struct Widths {
-  static constexpr int col = MODE == ENT_OFF16 ? 2 : 4;
-  static constexpr int cnt = MODE == ENT_PACKED ? 0 : (int)sizeof(CntT);
-};
-
-// L2 prefetch of group c: entry streams, R and perm (bulk prefetch, one lane)
-__device__ __forceinline__ void prefetch_group(const ViPack& P, int c, int col_bytes, int cnt_bytes) {
-  const int64_t s0 = __ldg(P.chunk_slot + c), s1 = __ldg(P.chunk_slot + c + 1);
-  const int64_t n = (s1 - s0) * 32;
-  if (n > 0) {
-    prefetch_l2(reinterpret_cast<const char*>(P.col) + s0 * 32 * col_bytes, (uint32_t)(n * col_bytes));
-    if (cnt_bytes)
-      prefetch_l2(reinterpret_cast<const char*>(P.cnt) + s0 * 32 * cnt_bytes, (uint32_t)(n * cnt_bytes));
-  }
-  prefetch_l2(P.R + (int64_t)c * kGroupRows, (uint32_t)(kGroupRows * 4));
-  prefetch_l2(P.perm + (int64_t)c * kGroupRows, (uint32_t)kGroupRows);
-}
-
-// VAR 0: 8 entries a batch, 5 CTAs per SM; VAR 1: 4 entries, 8 CTAs per SM
-// (latency hidden by more resident warps instead)
-template <int MODE, int VAR>
-struct MinBlocks {
-  static constexpr int value = MODE != ENT_PACKED ? 3 : (VAR == 0 ? 5 : 8);
-};
-template <int VAR>
-struct Batch {
-  static constexpr int value = VAR == 0 ? 8 : 4;
-};
-
-// One Jacobi sweep over groups [c_begin, c_end): warp per group, grid-stride;
-// prefetch bits: PF_NEXT = the warp's next group, PF_CURRENT = the group it starts.
+// One Jacobi sweep over chunks [c_begin, c_end): warp per chunk, grid-stride;
+// prefetch bits: PF_NEXT = the warp's next chunk, PF_CURRENT = the chunk it starts.
 template <int MODE, typename CntT, int VAR>
 __global__ void __launch_bounds__(kThreads, MinBlocks<MODE, VAR>::value)
     k_vi_chunks(ViPack P, int c_begin, int c_end, const float* __restrict__ Vin, float* Vout, int32_t* pi,
                 unsigned long long* resid, int prefetch) {
-  __shared__ float qs[kWarps][kQStride + 1];
-  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const int lane = threadIdx.x & 31;
   const int nw = gridDim.x * kWarps;
-  float* q = qs[wid];
   double dmax = 0.0;
-  for (int c = c_begin + blockIdx.x * kWarps + wid; c < c_end; c += nw) {
+  for (int c = c_begin + blockIdx.x * kWarps + (threadIdx.x >> 5); c < c_end; c += nw) {
     if ((prefetch & PF_NEXT) && lane == 0 && c + nw < c_end)
-      prefetch_group(P, c + nw, Widths<MODE, CntT>::col, Widths<MODE, CntT>::cnt);
-    if ((prefetch & PF_CURRENT) && lane == 0) prefetch_group(P, c, Widths<MODE, CntT>::col, Widths<MODE, CntT>::cnt);
-    const GroupPos gp = group_pos(P, c);
-    const float* Rg = P.R + (int64_t)c * kGroupRows;
-    group_q<MODE, CntT, false, Batch<VAR>::value>(P, c, gp, lane, 0, 1, Vin, q,
-                                                  [&](int pos, int, int) { return ld_stream(Rg + pos); });
-    __syncwarp();
-    group_argmax(P, gp, lane, q, [&](int sl, float bq, int ba) {
+      prefetch_chunk(P, c + nw, Widths<MODE, CntT>::col, Widths<MODE, CntT>::cnt);
+    if ((prefetch & PF_CURRENT) && lane == 0)
+      prefetch_chunk(P, c, Widths<MODE, CntT>::col, Widths<MODE, CntT>::cnt);
+    const ChunkPos cp = chunk_pos(P, c, lane, MODE != ENT_I32);
+    float bq = -INFINITY;
+    int ba = 0x7fffffff;
+    chunk_best<MODE, CntT, false, VAR>(P, c, cp, lane, 0, P.na, Vin, bq, ba, pack_r(P, c, 0, lane), 32);
+    if (cp.valid) {
       float vout;
       int32_t pout;
       finish_state(bq, ba, vout, pout);
-      const int64_t s = gp.s0 + sl;
-      if (resid) dmax = fmax(dmax, fabs((double)vout - (double)Vin[s]));
-      Vout[s] = vout;
-      pi[s] = pout;
-    });
-    __syncwarp();  // q is rewritten by the next group
+      if (resid) dmax = fmax(dmax, fabs((double)vout - (double)Vin[cp.s]));
+      Vout[cp.s] = vout;
+      pi[cp.s] = pout;
+    }
   }
   if (resid) {
-    for (int off = 16; off > 0; off >>= 1) dmax = fmax(dmax, __shfl_xor_sync(kFull, dmax, off));
+    for (int off = 16; off > 0; off >>= 1) dmax = fmax(dmax, __shfl_xor_sync(0xffffffffu, dmax, off));
     __shared__ double wmax[kWarps];
-    if (lane == 0) wmax[wid] = dmax;
+    if (lane == 0) wmax[threadIdx.x >> 5] = dmax;
     __syncthreads();
     if (threadIdx.x == 0) {
+      double mx = 0.0;
+      for (int w = 0; w < kWarps; ++w) mx = fmax(mx, wmax[w]);
+      if (mx > 0.0) atomicMax(resid, (unsigned long long)__double_as_longlong(mx));
+    }
+  }
+}
+
+// ---- TMA-staged Jacobi sweep (packed layout) ---------------------------------------
+// A CTA walks super-chunks of SC consecutive chunks; their entries, R and
+// per-action lengths are contiguous ranges of the sliced copy, so one thread
+// stages super-chunks NST-1 ahead with three 1-D bulk copies each
+// (cp.async.bulk, completion counted on an mbarrier per stage) into a ring of
+// NST shared-memory stages while the CTA computes: 8/SC warps per chunk,
+// each a block of actions, reading entries from shared memory
+// (conflict-free: lane l reads word l of a slot row) and gathering V through
+// L1.  DRAM latency is covered by the double buffer instead of by resident
+// warps.  A super-chunk whose entries exceed a stage is read from global
+// memory.  Waits are bounded (error bit 8 of err).
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return (uint32_t)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// 1-D bulk copy global -> this CTA's shared memory (no multicast); 16-byte
+// aligned addresses, size a multiple of 16
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+          smem_u32(dst)),
+      "l"(src), "r"(bytes), "r"(smem_u32(bar))
+      : "memory");
+}
+__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+__device__ __forceinline__ void fence_mbar_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
+
+template <int SC>
+__host__ __device__ __forceinline__ int sc_r_bytes(int na) { return SC * na * 32 * 4; }
+template <int SC>
+__host__ __device__ __forceinline__ int sc_ml_bytes(int na_pad) { return (SC * na_pad * 2 + 15) & ~15; }
+template <int SC, int EB>
+__host__ __device__ __forceinline__ int sc_stage_bytes(int na, int na_pad) {
+  return EB + sc_r_bytes<SC>(na) + sc_ml_bytes<SC>(na_pad);
+}
+
+template <int SC, int NST, int EB>
+__global__ void __launch_bounds__(kThreads)
+    k_vi_tma(ViPack P, int c_begin, int c_end, const float* __restrict__ Vin, float* Vout, int32_t* pi,
+             unsigned long long* resid, unsigned int* err) {
+  constexpr int kScChunks = SC;
+  constexpr int kScG = kWarps / SC;
+  constexpr int kScEntBytes = EB;
+  extern __shared__ __align__(128) unsigned char smem[];
+  __shared__ uint64_t bar[NST];
+  __shared__ int s_ok, s_direct[NST];
+  __shared__ float sq[kWarps][32];
+  __shared__ int sa[kWarps][32];
+  __shared__ double wmax[kWarps];
+  const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+  const int na = P.na, na_pad = P.na_pad;
+  const int stage_bytes = sc_stage_bytes<SC, EB>(na, na_pad);
+  const int n_sc = (c_end - c_begin + kScChunks - 1) / kScChunks;
+  const int cc = wid / kScG, grp = wid % kScG;
+  const int apg = (na + kScG - 1) / kScG;
+  const int a0 = min(na, grp * apg), a1 = min(na, a0 + apg);
+  const bool counts = P.count_type != VAL_F32;
+
+  auto issue = [&](int sc, int st) {  // thread 0
+    const int c0 = c_begin + sc * kScChunks, c1 = min(c0 + kScChunks, c_end);
+    const int64_t e0 = __ldg(P.chunk_slot + c0), e1 = __ldg(P.chunk_slot + c1);
+    const int64_t eb = (e1 - e0) * 128;
+    unsigned char* sp = smem + st * stage_bytes;
+    if (eb > kScEntBytes) {  // too large for a stage: read from global memory
+      s_direct[st] = 1;
+      mbar_expect_tx(&bar[st], 0);
+      return;
+    }
+    s_direct[st] = 0;
+    const uint32_t rb = (uint32_t)((c1 - c0) * na * 128);
+    const uint32_t mb = (uint32_t)((c1 - c0) * na_pad * 2);
+    mbar_expect_tx(&bar[st], (uint32_t)eb + rb + mb);
+    if (eb) bulk_g2s(sp, reinterpret_cast<const char*>(P.col) + e0 * 128, (uint32_t)eb, &bar[st]);
+    bulk_g2s(sp + kScEntBytes, P.R + (int64_t)c0 * na * 32, rb, &bar[st]);
+    bulk_g2s(sp + kScEntBytes + sc_r_bytes<SC>(na), P.maxlen + (int64_t)c0 * na_pad, mb, &bar[st]);
+  };
+
+  if (tid == 0) {
+    for (int q = 0; q < NST; ++q) mbar_init(&bar[q], 1);
+    fence_mbar_init();
+  }
+  __syncthreads();
+  int sc = blockIdx.x;
+  if (tid == 0)
+    for (int q = 0; q < NST - 1; ++q)
+      if (sc + q * (int)gridDim.x < n_sc) issue(sc + q * gridDim.x, q);
+  double dmax = 0.0;
+  bool failed = false;
+  for (int k = 0; sc < n_sc; ++k, sc += gridDim.x) {
+    const int st = k % NST;
+    if (tid == 0) {
+      const int ahead = sc + (NST - 1) * (int)gridDim.x;
+      if (ahead < n_sc) {
+        fence_proxy_async();  // that stage was read through the generic proxy
+        issue(ahead, (k + NST - 1) % NST);
+      }
+      long long it = 0;
+      const uint32_t parity = (uint32_t)((k / NST) & 1);
+      while (!mbar_try_wait(&bar[st], parity) && ++it < (1ll << 24)) {
+      }
+      s_ok = it < (1ll << 24);
+    }
+    __syncthreads();
+    if (!s_ok) {
+      if (tid == 0) atomicOr(err, 8u);
+      failed = true;
+      break;
+    }
+    const int c0 = c_begin + sc * kScChunks;
+    const int c = c0 + cc;
+    const bool active = c < c_end;
+    float bq = -INFINITY;
+    int ba = 0x7fffffff;
+    ChunkPos cp{0, 0, false};
+    if (active) {
+      cp = chunk_pos(P, c, lane, true);
+      if (s_direct[st]) {
+        chunk_best<ENT_PACKED, uint16_t, false, 1>(P, c, cp, lane, a0, a1, Vin, bq, ba, pack_r(P, c, a0, lane), 32);
+      } else {
+        const unsigned char* sp = smem + st * stage_bytes;
+        const uint32_t* ent = reinterpret_cast<const uint32_t*>(sp);
+        const float* Rs = reinterpret_cast<const float*>(sp + kScEntBytes);
+        const uint16_t* mls = reinterpret_cast<const uint16_t*>(sp + kScEntBytes + sc_r_bytes<SC>(na)) + cc * na_pad;
+        int64_t slot = __ldg(P.chunk_slot + c) - __ldg(P.chunk_slot + c0);
+        for (int b = 0; b < a0; ++b) slot += mls[b];
+        const uint32_t* ep = ent + slot * 32 + lane;
+        const float* rp = Rs + ((int64_t)cc * na + a0) * 32 + lane;
+        const float* vb = Vin + cp.base;
+        for (int a = a0; a < a1; ++a) {
+          const int ml = mls[a];
+          float acc = 0.f;
+          for (int k0 = 0; k0 < ml; k0 += 4) {
+            const int n = min(ml - k0, 4);
+            uint32_t e[4];
+            float v[4];
+#pragma unroll
+            for (int j = 0; j < 4; ++j) e[j] = j < n ? ep[(k0 + j) * 32] : 0u;
+#pragma unroll
+            for (int j = 0; j < 4; ++j) v[j] = j < n ? __ldg(vb + (e[j] & 0xffffu)) : 0.f;
+#pragma unroll
+            for (int j = 0; j < 4; ++j) acc = fmaf((float)(e[j] >> 16), v[j], acc);  // padding: exact no-op
+          }
+          ep += ml * 32;
+          const float q = finish_row(*rp, acc, 0.f, P.nrzns, counts);
+          rp += 32;
+          if (!isnan(q) && q > bq) {
+            bq = q;
+            ba = a;
+          }
+        }
+      }
+    }
+    sq[wid][lane] = bq;
+    sa[wid][lane] = ba;
+    __syncthreads();  // candidates in place; the stage is consumed
+    if (active && grp == 0) {
+      for (int g2 = 1; g2 < kScG; ++g2) {
+        const float oq = sq[wid + g2][lane];
+        if (oq > bq) {  // later groups hold later actions: strict '>' keeps the first maximum
+          bq = oq;
+          ba = sa[wid + g2][lane];
+        }
+      }
+      if (cp.valid) {
+        float vout;
+        int32_t pout;
+        finish_state(bq, ba, vout, pout);
+        if (resid) dmax = fmax(dmax, fabs((double)vout - (double)Vin[cp.s]));
+        Vout[cp.s] = vout;
+        pi[cp.s] = pout;
+      }
+    }
+    __syncthreads();  // sq/sa free for the next super-chunk
+  }
+  if (failed && tid == 0) {
+    // give the copies in flight time to land before the CTA exits
+    for (int st = 0; st < NST; ++st) {
+      long long it = 0;
+      while (!mbar_try_wait(&bar[st], 0) && !mbar_try_wait(&bar[st], 1) && ++it < (1ll << 24)) {
+      }
+    }
+  }
+  if (resid) {
+    for (int off = 16; off > 0; off >>= 1) dmax = fmax(dmax, __shfl_xor_sync(0xffffffffu, dmax, off));
+    if (lane == 0) wmax[wid] = dmax;
+    __syncthreads();
+    if (tid == 0) {
       double mx = 0.0;
       for (int w = 0; w < kWarps; ++w) mx = fmax(mx, wmax[w]);
       if (mx > 0.0) atomicMax(resid, (unsigned long long)__double_as_longlong(mx));
@@ -447,47 +578,58 @@ __device__ __forceinline__ bool grid_barrier(unsigned int* sync, unsigned int ta
 // The layered (backward-induction) schedule in one persistent launch: layer
 // nlayers-1 first (V = max_a R), then layers down to 0, each reading the V of
 // the layer after it, with a grid barrier between layers.  `groups` warps
-// share a group of states, each taking every groups-th slice; their rows' Q
-// meet in shared memory and the first warp takes the argmax.  With PF_NEXT,
-// each group's data for the next layer is prefetched into L2 before this
-// layer's work, so HBM streams layer t-1 while layer t computes.
+// share a chunk, each taking a contiguous block of actions; their candidates
+// are combined in action order through shared memory.  With PF_NEXT, each
+// chunk's data for the next layer is prefetched into L2 before this layer's
+// work, so HBM streams layer t-1 while layer t computes.
 template <int MODE, typename CntT, int VAR>
 __global__ void __launch_bounds__(kThreads, MinBlocks<MODE, VAR>::value)
     k_vi_layered(ViPack P, int groups, float* V, int32_t* pi, unsigned int* sync, int prefetch, WaitBound wb) {
-  __shared__ float qs[kWarps][kQStride + 1];
+  __shared__ float sq[kWarps][32];
+  __shared__ int sa[kWarps][32];
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  const int cpc = kWarps / groups;  // groups of states per CTA iteration
+  const int cpc = kWarps / groups;  // chunks per CTA iteration
   const int grp = wid % groups, slot_in_cta = wid / groups;
-  float* q = qs[slot_in_cta];
+  const int apg = (P.na + groups - 1) / groups;
+  const int a0 = min(P.na, grp * apg), a1 = min(P.na, a0 + apg);
   const int cpl = (int)P.cpl;
   unsigned int gen = 0;
   for (int t = P.nlayers - 1; t >= 0; --t) {
     for (int b = blockIdx.x * cpc; b < cpl; b += gridDim.x * cpc) {
       const int cc = b + slot_in_cta;
       const bool active = cc < cpl;
-      const int c = t * cpl + cc;
-      GroupPos gp{0, 0, 0, 0, 0};
+      float bq = -INFINITY;
+      int ba = 0x7fffffff;
+      ChunkPos cp{0, 0, false};
       if (active) {
+        const int c = t * cpl + cc;
         if ((prefetch & PF_NEXT) && lane == 0 && grp == 0 && t > 0)
-          prefetch_group(P, c - cpl, Widths<MODE, CntT>::col, Widths<MODE, CntT>::cnt);
-        gp = group_pos(P, c);
-        const float* Rg = P.R + (int64_t)c * kGroupRows;
-        group_q<MODE, CntT, true, Batch<VAR>::value>(P, c, gp, lane, grp, groups, V, q,
-                                                     [&](int pos, int, int) { return ld_stream(Rg + pos); });
+          prefetch_chunk(P, c - cpl, Widths<MODE, CntT>::col, Widths<MODE, CntT>::cnt);
+        cp = chunk_pos(P, c, lane, MODE != ENT_I32);
+        chunk_best<MODE, CntT, true, VAR>(P, c, cp, lane, a0, a1, V, bq, ba, pack_r(P, c, a0, lane), 32);
       }
-      if (groups > 1) __syncthreads();
-      else __syncwarp();
-      if (active && grp == 0) {
-        group_argmax(P, gp, lane, q, [&](int sl, float bq, int ba) {
-          float vout;
-          int32_t pout;
-          finish_state(bq, ba, vout, pout);
-          V[gp.s0 + sl] = vout;
-          pi[gp.s0 + sl] = pout;
-        });
+      if (groups > 1) {
+        sq[wid][lane] = bq;
+        sa[wid][lane] = ba;
+        __syncthreads();
+        if (active && grp == 0) {
+          for (int g2 = 1; g2 < groups; ++g2) {
+            const float oq = sq[wid + g2][lane];
+            if (oq > bq) {  // later groups hold later actions: strict '>' keeps the first maximum
+              bq = oq;
+              ba = sa[wid + g2][lane];
+            }
+          }
+        }
+        __syncthreads();
       }
-      if (groups > 1) __syncthreads();
-      else __syncwarp();
+      if (active && grp == 0 && cp.valid) {
+        float vout;
+        int32_t pout;
+        finish_state(bq, ba, vout, pout);
+        V[cp.s] = vout;
+        pi[cp.s] = pout;
+      }
     }
     if (t > 0) {
       ++gen;
@@ -498,18 +640,18 @@ __global__ void __launch_bounds__(kThreads, MinBlocks<MODE, VAR>::value)
 
 // Many layered solves in one persistent launch.  Step k covers layer
 // nlayers-1-k of every job that has more than k layers (jobs sorted by layer
-// count, so those are a prefix and their groups a contiguous item range).
-// There is no grid-wide barrier: a group of layer t waits only until its own
-// job's layer t+1 is complete (done[job][t+1] == groups per layer), and each
-// finished group adds one to done[job][t].  Every CTA takes its items in step
+// count, so those are a prefix and their chunks a contiguous item range).
+// There is no grid-wide barrier: a chunk of layer t waits only until its own
+// job's layer t+1 is complete (done[job][t+1] == chunks per layer), and each
+// finished chunk adds one to done[job][t].  Every CTA takes its items in step
 // order and all CTAs are resident (cooperative launch), so each wait is for
 // items of an earlier step that are finished or running; the waits are
 // bounded and a timeout sets bit 2 of err and lets the rest drain quickly.
-// Jobs with a target take R of the cells around it from their Rwin table,
-// and the target's own cells are terminal: the reference leaves such a
-// sample in place with reward 0 (src/build_model.cu:523-545), i.e. one entry
-// (the cell at t+1, count nrzns) and R = 0, evaluated here with the same
-// operations as that row.
+// Jobs with a target take R of the
+// cells around it from their Rwin table, and the target's own cells are
+// terminal: the reference leaves such a sample in place with reward 0
+// (src/build_model.cu:523-545), i.e. one entry (the cell at t+1, count
+// nrzns) and R = 0, evaluated here with the same operations as that row.
 template <int MODE, int VAR>
 struct BatchMinBlocks {  // the job lookup needs a few more registers than k_vi_layered
   static constexpr int value = MODE != ENT_PACKED ? 3 : (VAR == 0 ? 4 : 5);
@@ -519,7 +661,8 @@ template <int MODE, typename CntT, int VAR>
 __global__ void __launch_bounds__(kThreads, BatchMinBlocks<MODE, VAR>::value)
     k_vi_batch(const unsigned char* table, int job_cap, int groups, int* done, int layer_cap,
                unsigned int* err, int prefetch, WaitBound wb) {
-  __shared__ float qs[kWarps][kQStride + 1];
+  __shared__ float sq[kWarps][32];
+  __shared__ int sa[kWarps][32];
   const ViBatchHeader* H = reinterpret_cast<const ViBatchHeader*>(table);
   const ViJob* jobs = reinterpret_cast<const ViJob*>(table + kViBatchJobsOffset);
   const int* cum = reinterpret_cast<const int*>(jobs + job_cap);
@@ -528,17 +671,20 @@ __global__ void __launch_bounds__(kThreads, BatchMinBlocks<MODE, VAR>::value)
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   const int cpc = kWarps / groups;
   const int grp = wid % groups, slot_in_cta = wid / groups;
-  float* q = qs[slot_in_cta];
   for (int k = 0; k < L; ++k) {
     const int nj = nact[k];
     const int n_items = cum[nj];
     for (int b = blockIdx.x * cpc; b < n_items; b += gridDim.x * cpc) {
       const int item = b + slot_in_cta;
       const bool active = item < n_items;
-      int jid = 0, c = 0, t = 0;
+      float bq = -INFINITY;
+      int ba = 0x7fffffff;
+      bool valid = false;
+      float* Vout = nullptr;
+      int32_t* pout = nullptr;
+      int64_t s_out = 0;
       int* done_slot = nullptr;
       bool skip = false;
-      GroupPos gp{0, 0, 0, 0, 0};
       if (active) {
         int lo = 0, hi = nj - 1;  // last job with cum[job] <= item
         while (lo < hi) {
@@ -546,15 +692,18 @@ __global__ void __launch_bounds__(kThreads, BatchMinBlocks<MODE, VAR>::value)
           if (__ldg(cum + mid) <= item) lo = mid;
           else hi = mid - 1;
         }
-        jid = lo;
-        const ViJob& J = jobs[jid];
+        const ViJob& J = jobs[lo];
         const ViPack& P = J.P;
-        const int cpl = (int)P.cpl;
-        t = P.nlayers - 1 - k;
-        c = t * cpl + (item - __ldg(cum + jid));
-        done_slot = done + (int64_t)jid * layer_cap + t;
+        const int na = P.na;
+        const int apg = (na + groups - 1) / groups;
+        int a0 = min(na, grp * apg);
+        const int a1 = min(na, a0 + apg);
+        const int cpl = (int)P.cpl, nc = (int)P.nc;
+        const int t = P.nlayers - 1 - k;
+        const int c = t * cpl + (item - __ldg(cum + lo));
+        done_slot = done + (int64_t)lo * layer_cap + t;
         if ((prefetch & PF_NEXT) && lane == 0 && grp == 0 && t > 0)
-          prefetch_group(P, c - cpl, Widths<MODE, CntT>::col, Widths<MODE, CntT>::cnt);
+          prefetch_chunk(P, c - cpl, Widths<MODE, CntT>::col, Widths<MODE, CntT>::cnt);
         if (t + 1 < P.nlayers) {  // layer t+1 of this job complete
           const int* dep = done_slot + 1;
           int ok = 1;
@@ -570,190 +719,136 @@ __global__ void __launch_bounds__(kThreads, BatchMinBlocks<MODE, VAR>::value)
               __nanosleep(64);
             }
           }
-          ok = __shfl_sync(kFull, ok, 0);
+          ok = __shfl_sync(0xffffffffu, ok, 0);
           (void)ld_acquire_s32(dep);  // every lane orders its reads after the producers' writes
-          skip = !ok;                 // give up this group: nothing computed, nothing written
+          if (!ok) {
+            skip = true;  // give up this chunk: nothing computed, nothing written
+            a0 = a1;
+          }
         }
-        gp = group_pos(P, c);
-        if (!skip) {
-          const float* Rg = P.R + (int64_t)c * kGroupRows;
-          const bool win = J.Rwin && t + 1 < P.nlayers;
-          const int na = P.na;
-          group_q<MODE, CntT, true, Batch<VAR>::value>(
-              P, c, gp, lane, grp, groups, J.V, q, [&](int pos, int s_local, int a) {
-                const int sl = gp.sl0 + s_local;
-                if (win && sl >= J.wi0 * P.g && sl < (J.wi0 + J.wh) * P.g) {
-                  const int i = sl / P.g, jj = sl - i * P.g;
-                  const int wi = i - J.wi0, wj = jj - J.wj0;
-                  if (wj >= 0 && wj < J.ww)
-                    return ld_stream(J.Rwin + (((int64_t)t * J.wh + wi) * J.ww + wj) * na + a);
-                }
-                return ld_stream(Rg + pos);
-              });
+        const ChunkPos cp = chunk_pos(P, c, lane, MODE != ENT_I32);
+        const float* Rp = pack_r(P, c, a0, lane);
+        int rstride = 32;
+        bool terminal = false;
+        if (J.Rwin && cp.valid && t + 1 < P.nlayers) {
+          const int sl = (int)(cp.s - (int64_t)t * nc);
+          const int i = sl / P.g, j = sl - (sl / P.g) * P.g;
+          terminal = i >= J.ti && i < J.ti + J.tsg && j >= J.tj && j < J.tj + J.tsg;
+          const int wi = i - J.wi0, wj = j - J.wj0;
+          if (wi >= 0 && wi < J.wh && wj >= 0 && wj < J.ww) {
+            Rp = J.Rwin + (((int64_t)t * J.wh + wi) * J.ww + wj) * na + a0;
+            rstride = 1;
+          }
         }
+        chunk_best<MODE, CntT, true, VAR>(P, c, cp, lane, a0, a1, J.V, bq, ba, Rp, rstride);
+        if (terminal) {
+          const float v = ld_value<true>(J.V + cp.s + nc);  // the same cell, layer t+1
+          const float acc = fmaf((float)P.nrzns, v, 0.f);
+          const float q = finish_row(0.f, acc, 0.f, P.nrzns, true);
+          bq = -INFINITY;
+          ba = 0x7fffffff;
+          if (a0 < a1 && !isnan(q)) {
+            bq = q;
+            ba = a0;
+          }
+        }
+        valid = cp.valid && !skip;
+        Vout = J.V;
+        pout = J.pi;
+        s_out = cp.s;
       }
-      if (groups > 1) __syncthreads();
-      else __syncwarp();
-      if (active && grp == 0) {
-        const ViJob& J = jobs[jid];
-        const ViPack& P = J.P;
-        if (!skip) {
-          const int nc = (int)P.nc;
-          group_argmax(P, gp, lane, q, [&](int sl, float bq, int ba) {
-            const int64_t s = gp.s0 + sl;
-            if (J.Rwin && t + 1 < P.nlayers) {
-              const int cl = gp.sl0 + sl;
-              const int i = cl / P.g, j = cl - (cl / P.g) * P.g;
-              if (i >= J.ti && i < J.ti + J.tsg && j >= J.tj && j < J.tj + J.tsg) {
-                const float v = ld_value<true>(J.V + s + nc);  // the same cell, layer t+1
-                const float acc = fmaf((float)P.nrzns, v, 0.f);
-                const float qt = finish_row(0.f, acc, 0.f, P.nrzns, true);
-                bq = -INFINITY;
-                ba = 0x7fffffff;
-                if (!isnan(qt)) {
-                  bq = qt;
-                  ba = 0;
-                }
-              }
+      if (groups > 1) {
+        sq[wid][lane] = bq;
+        sa[wid][lane] = ba;
+        __syncthreads();
+        if (active && grp == 0) {
+          for (int g2 = 1; g2 < groups; ++g2) {
+            const float oq = sq[wid + g2][lane];
+            if (oq > bq) {  // later groups hold later actions: strict '>' keeps the first maximum
+              bq = oq;
+              ba = sa[wid + g2][lane];
             }
-            float vout;
-            int32_t po;
-            finish_state(bq, ba, vout, po);
-            J.V[s] = vout;
-            J.pi[s] = po;
-          });
+          }
+        }
+        __syncthreads();
+      }
+      if (active && grp == 0) {
+        if (valid) {
+          float vout;
+          int32_t po;
+          finish_state(bq, ba, vout, po);
+          Vout[s_out] = vout;
+          pout[s_out] = po;
         }
         __syncwarp();
         if (lane == 0) {
-          __threadfence();  // this group's values before its completion count
+          __threadfence();  // this chunk's values before its completion count
           atomicAdd(done_slot, 1);
         }
       }
-      if (groups > 1) __syncthreads();
-      else __syncwarp();
     }
   }
 }
 
 // ---- pack construction ------------------------------------------------------------
 
-// Per group (warp per group): the rows' lengths, their order (longest first,
-// stable; a counting sort on min(len, 63)), perm and R in that order, the
-// slices' maxlen and their sum.
+// per chunk: maxlen of every action over the chunk's 32 rows, and their sum
 template <typename PtrT>
 __global__ void __launch_bounds__(kThreads) k_pack_count(ViModel M, ViPack P, int32_t* slot_len,
-                                                         uint16_t* maxlen, uint8_t* perm, float* Rs) {
-  __shared__ int lens[kWarps][kGroupRows];
-  __shared__ int slen[kWarps][kGroupRows];
-  __shared__ int off[kWarps][kLenKeys];
-  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  const int c = blockIdx.x * kWarps + wid;
-  if (c >= P.nchunks) return;  // warp-level work only: no block barrier below
-  const GroupPos gp = group_pos(P, c);
-  const PtrT* rp = reinterpret_cast<const PtrT*>(M.row_ptr);
-  const int na = P.na;
-  for (int r = lane; r < kGroupRows; r += 32) {
-    int len = 0;
-    if (r < gp.rows) {
-      const int64_t s = gp.s0 + r / na;
-      if (s < P.n_row_states) {
-        const int64_t row = s * na + (r % na);
-        len = (int)((int64_t)rp[row + 1] - (int64_t)rp[row]);
-      }
-    }
-    lens[wid][r] = len;
-  }
-  for (int k = lane; k < kLenKeys; k += 32) off[wid][k] = 0;
-  __syncwarp();
-  // key 0 = longest rows
-  auto key_of = [](int len) { return kLenKeys - 1 - min(len, kLenKeys - 1); };
-  for (int r = lane; r < gp.rows; r += 32) atomicAdd(&off[wid][key_of(lens[wid][r])], 1);
-  __syncwarp();
-  {  // exclusive prefix of the key counts, two keys a lane
-    const int v0 = off[wid][2 * lane], v1 = off[wid][2 * lane + 1];
-    int incl = v0 + v1;
-    for (int o = 1; o < 32; o <<= 1) {
-      const int t2 = __shfl_up_sync(kFull, incl, o);
-      if (lane >= o) incl += t2;
-    }
-    const int ex = incl - v0 - v1;
-    __syncwarp();
-    off[wid][2 * lane] = ex;
-    off[wid][2 * lane + 1] = ex + v0;
-  }
-  __syncwarp();
-  // stable placement, 32 rows at a time, rows of equal length in
-  // action-major order (u = a * gvalid + s_local): a slice then holds few
-  // actions over consecutive states, whose V gathers share cache lines
-  for (int base = 0; base < gp.rows; base += 32) {
-    const int u = base + lane;
-    const bool has = u < gp.rows;
-    const int ua = has ? u / gp.gvalid : 0;
-    const int r = has ? (u - ua * gp.gvalid) * na + ua : 0;
-    const int key = has ? key_of(lens[wid][r]) : kLenKeys + lane;
-    const unsigned m = __match_any_sync(kFull, key);
-    const int rank = __popc(m & ((1u << lane) - 1u));
-    const int pos = has ? off[wid][key] + rank : 0;
-    __syncwarp();
-    if (has && rank == 0) off[wid][key] += __popc(m);
-    __syncwarp();
-    if (has) {
-      perm[(int64_t)c * kGroupRows + pos] = (uint8_t)r;
-      slen[wid][pos] = lens[wid][r];
-      Rs[(int64_t)c * kGroupRows + pos] = M.R[(gp.s0 + r / na) * na + (r % na)];
-    }
-  }
-  __syncwarp();
-  for (int pos = gp.rows + lane; pos < kGroupRows; pos += 32) {
-    perm[(int64_t)c * kGroupRows + pos] = 0;
-    Rs[(int64_t)c * kGroupRows + pos] = 0.f;
-  }
-  int total = 0;
-  for (int j = 0; j < kSlices; ++j) {
-    const int pos = (j << 5) + lane;
-    const unsigned ml = __reduce_max_sync(kFull, pos < gp.rows ? (unsigned)slen[wid][pos] : 0u);
-    if (lane == 0) maxlen[(int64_t)c * kSlices + j] = (uint16_t)ml;
-    total += (int)ml;
-  }
-  if (lane == 0) slot_len[c] = total;
-}
-
-// scatter the CSR rows into the group layout; flags[0] |= 1 when a window
-// offset does not fit 16 bits (the caller then packs with int32 columns)
-template <typename PtrT, int MODE, typename CntT>
-__global__ void __launch_bounds__(kThreads) k_pack_fill(ViModel M, ViPack P, void* colv, CntT* cnt,
-                                                        unsigned int* flags) {
+                                                         uint16_t* maxlen) {
   const int lane = threadIdx.x & 31;
   const int c = blockIdx.x * kWarps + (threadIdx.x >> 5);
   if (c >= P.nchunks) return;
-  const GroupPos gp = group_pos(P, c);
+  const ChunkPos cp = chunk_pos(P, c, lane, false);
+  const bool has = cp.valid && cp.s < P.n_row_states;
+  const PtrT* rp = reinterpret_cast<const PtrT*>(M.row_ptr);
+  int64_t prev = has ? (int64_t)rp[cp.s * P.na] : 0;
+  int total = 0;
+  for (int a = 0; a < P.na; ++a) {
+    unsigned len = 0;
+    if (has) {
+      const int64_t nx = (int64_t)rp[cp.s * P.na + a + 1];
+      len = (unsigned)(nx - prev);
+      prev = nx;
+    }
+    const unsigned ml = __reduce_max_sync(0xffffffffu, len);
+    if (lane == 0) maxlen[(int64_t)c * P.na_pad + a] = (uint16_t)ml;
+    total += (int)ml;
+  }
+  if (lane == 0) {
+    for (int a = P.na; a < P.na_pad; ++a) maxlen[(int64_t)c * P.na_pad + a] = 0;
+    slot_len[c] = total;
+  }
+}
+
+// scatter the CSR rows into the chunk layout; flags[0] |= 1 when a window
+// offset does not fit 16 bits (the caller then packs with int32 columns)
+template <typename PtrT, int MODE, typename CntT>
+__global__ void __launch_bounds__(kThreads) k_pack_fill(ViModel M, ViPack P, void* colv, CntT* cnt,
+                                                        float* Rp, unsigned int* flags) {
+  const int lane = threadIdx.x & 31;
+  const int c = blockIdx.x * kWarps + (threadIdx.x >> 5);
+  if (c >= P.nchunks) return;
+  const ChunkPos cp = chunk_pos(P, c, lane, MODE != ENT_I32);
+  const bool has = cp.valid && cp.s < P.n_row_states;
   const PtrT* rp = reinterpret_cast<const PtrT*>(M.row_ptr);
   const CntT* src = reinterpret_cast<const CntT*>(M.cnt);
-  const int na = P.na;
   int64_t slot = P.chunk_slot[c];
   bool bad = false;
-  for (int j = 0; j < kSlices; ++j) {
-    const int ml = P.maxlen[(int64_t)c * kSlices + j];
-    const int pos = (j << 5) + lane;
-    const bool valid = pos < gp.rows;
-    const int r = valid ? P.perm[(int64_t)c * kGroupRows + pos] : 0;
-    int s_local, a;
-    row_of(P, r, s_local, a);
-    const int64_t s = gp.s0 + s_local;
-    const bool has = valid && s < P.n_row_states;
+  // lanes without rows gather nothing that is kept; give them a valid index too
+  const int32_t pad_col = !has ? 0 : (int32_t)(cp.s / P.nc + 1 < P.nlayers ? cp.s + P.nc : cp.s);
+  for (int a = 0; a < P.na; ++a) {
+    const int ml = P.maxlen[(int64_t)c * P.na_pad + a];
     int64_t rs = 0, len = 0;
     if (has) {
-      const int64_t row = s * na + a;
-      rs = (int64_t)rp[row];
-      len = (int64_t)rp[row + 1] - rs;
+      rs = (int64_t)rp[cp.s * P.na + a];
+      len = (int64_t)rp[cp.s * P.na + a + 1] - rs;
     }
-    const int64_t base = MODE == ENT_I32 ? 0 : window_base(P, s);
-    // padding (count 0) points at the row's own cell in layer t+1, finished
-    // before layer t in every schedule, so the gathered value is finite and
-    // fma(0, v, acc) leaves acc unchanged; unused lanes get the same index
-    const int32_t pad_col = (int32_t)(gp.t + 1 < P.nlayers ? s + P.nc : s);
     for (int k = 0; k < ml; ++k) {
       const int64_t e = (slot + k) * 32 + lane;
+      // padding (count 0) points at the lane's own cell in layer t+1, finished
+      // before layer t in every schedule, so the gathered value is finite and
+      // fma(0, v, acc) leaves acc unchanged
       int32_t col = pad_col;
       CntT w = 0;
       if (k < len) {
@@ -764,9 +859,9 @@ __global__ void __launch_bounds__(kThreads) k_pack_fill(ViModel M, ViPack P, voi
         reinterpret_cast<int32_t*>(colv)[e] = col;
         cnt[e] = w;
       } else {
-        int64_t o = (int64_t)col - base;
+        int64_t o = (int64_t)col - cp.base;
         if (o < 0 || o > 65535) {
-          if (valid) bad = true;
+          bad = true;
           o = 0;
         }
         if (MODE == ENT_PACKED) {
@@ -778,6 +873,7 @@ __global__ void __launch_bounds__(kThreads) k_pack_fill(ViModel M, ViPack P, voi
       }
     }
     slot += ml;
+    Rp[((int64_t)c * P.na + a) * 32 + lane] = cp.valid ? M.R[cp.s * P.na + a] : 0.f;
   }
   if (bad) atomicOr(flags, 1u);
 }
@@ -835,9 +931,9 @@ void free_pack(PackStore* p) {
 }
 
 int64_t pack_sweep_bytes(const ViPack& P) {
-  // entries (with padding) + R + perm + group tables + V read + V' and policy written
-  return P.slot_rows * 32 * (col_bytes_of(P) + cnt_bytes_of(P)) + P.nchunks * kGroupRows * (4 + 1) +
-         P.nchunks * (8 + kSlices * 2) + P.ns * 12;
+  // entries (with padding) + R + chunk tables + V read + V' and policy written
+  return P.slot_rows * 32 * (col_bytes_of(P) + cnt_bytes_of(P)) + P.nchunks * P.na * 32 * 4 +
+         P.nchunks * (8 + P.na_pad * 2) + P.ns * 12;
 }
 
 cudaError_t build_pack(const ViModel& M, int64_t nc, int g, int del, PackStore* out, cudaStream_t st) {
@@ -846,26 +942,17 @@ cudaError_t build_pack(const ViModel& M, int64_t nc, int g, int del, PackStore* 
   P.ns = M.ns;
   P.nc = (nc > 0 && M.ns % nc == 0) ? nc : M.ns;
   P.nlayers = (int)(M.ns / P.nc);
-  P.na = M.na;
-  if (P.na < 1 || P.na > kGroupRows) return cudaErrorInvalidValue;
-  P.gs = std::max(1, kGroupRows / P.na);
-  P.cpl = (P.nc + P.gs - 1) / P.gs;
+  P.cpl = (P.nc + 31) / 32;
   P.nchunks = P.cpl * P.nlayers;
   if (P.nc >= ((int64_t)1 << 31) - 64 || P.nchunks >= ((int64_t)1 << 31) - 1)
-    return cudaErrorInvalidValue;  // 32-bit group arithmetic
+    return cudaErrorInvalidValue;  // 32-bit chunk arithmetic
   P.n_row_states = M.n_row_states;
+  P.na = M.na;
   P.na_pad = (M.na + 7) & ~7;
   P.nrzns = M.nrzns;
   P.count_type = M.count_type;
   P.g = g;
   P.del = del;
-  P.delg = (int64_t)del * (g + 1);
-  P.na_shift = -1;
-  for (int k = 0; k < 9; ++k)
-    if (P.na == (1 << k)) P.na_shift = k;
-  P.lps = 1;
-  while (P.lps * 2 * P.gs <= 32) P.lps *= 2;
-  P.apl = (P.na + P.lps - 1) / P.lps;
   const bool window =
       P.nlayers > 1 && g > 0 && (int64_t)g * g == P.nc && (int64_t)(2 * del) * (g + 1) <= 65535;
   P.ent_mode = !window ? ENT_I32 : (M.count_type == CNT_U16 ? ENT_PACKED : ENT_OFF16);
@@ -881,23 +968,17 @@ cudaError_t build_pack(const ViModel& M, int64_t nc, int g, int del, PackStore* 
   };
   const int64_t nb = (P.nchunks + 1023) / 1024 + 1;
   if ((e = dalloc(&out->bufs[0], sizeof(int64_t) * (P.nchunks + 1), st)) != cudaSuccess) return e;
-  if ((e = dalloc(&out->bufs[1], sizeof(uint16_t) * P.nchunks * kSlices, st)) != cudaSuccess) return e;
-  if ((e = dalloc(&out->bufs[4], sizeof(float) * (size_t)(P.nchunks * kGroupRows), st)) != cudaSuccess) return e;
-  if ((e = dalloc(&out->bufs[5], (size_t)(P.nchunks * kGroupRows), st)) != cudaSuccess) return e;
+  if ((e = dalloc(&out->bufs[1], sizeof(uint16_t) * P.nchunks * P.na_pad, st)) != cudaSuccess) return e;
   if ((e = dalloc((void**)&slot_len, sizeof(int32_t) * P.nchunks, st)) != cudaSuccess) return cleanup(), e;
   if ((e = dalloc((void**)&block_sums, sizeof(int64_t) * nb, st)) != cudaSuccess) return cleanup(), e;
   if ((e = dalloc((void**)&flags, sizeof(unsigned int) * 2, st)) != cudaSuccess) return cleanup(), e;
   P.chunk_slot = (const int64_t*)out->bufs[0];
   P.maxlen = (const uint16_t*)out->bufs[1];
-  P.R = (const float*)out->bufs[4];
-  P.perm = (const uint8_t*)out->bufs[5];
   const unsigned blocks = (unsigned)((P.nchunks + kWarps - 1) / kWarps);
   if (M.index_bits == 32)
-    k_pack_count<int32_t><<<blocks, kThreads, 0, st>>>(M, P, slot_len, (uint16_t*)out->bufs[1],
-                                                       (uint8_t*)out->bufs[5], (float*)out->bufs[4]);
+    k_pack_count<int32_t><<<blocks, kThreads, 0, st>>>(M, P, slot_len, (uint16_t*)out->bufs[1]);
   else
-    k_pack_count<int64_t><<<blocks, kThreads, 0, st>>>(M, P, slot_len, (uint16_t*)out->bufs[1],
-                                                       (uint8_t*)out->bufs[5], (float*)out->bufs[4]);
+    k_pack_count<int64_t><<<blocks, kThreads, 0, st>>>(M, P, slot_len, (uint16_t*)out->bufs[1]);
   if ((e = cudaGetLastError()) != cudaSuccess) return cleanup(), e;
   int64_t* cs = (int64_t*)out->bufs[0];
   if ((e = launch_scan_tiles(slot_len, P.nchunks, cs, cs + P.nchunks, block_sums, st)) != cudaSuccess)
@@ -908,6 +989,9 @@ cudaError_t build_pack(const ViModel& M, int64_t nc, int g, int del, PackStore* 
     return cleanup(), e;
   if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return cleanup(), e;
   P.slot_rows = slot_rows;
+  if ((e = dalloc(&out->bufs[4], sizeof(float) * (size_t)(P.nchunks * P.na * 32), st)) != cudaSuccess)
+    return cleanup(), e;
+  P.R = (const float*)out->bufs[4];
   for (int attempt = 0; attempt < 2; ++attempt) {
     const int cb = col_bytes_of(P), nb2 = cnt_bytes_of(P);
     // 16 spare elements keep every bulk prefetch inside its allocation
@@ -922,11 +1006,11 @@ cudaError_t build_pack(const ViModel& M, int64_t nc, int g, int del, PackStore* 
       using CntT = std::remove_pointer_t<decltype(cntt)>;
       constexpr int MODE = decltype(mode)::value;
       if (M.index_bits == 32)
-        k_pack_fill<int32_t, MODE, CntT><<<blocks, kThreads, 0, st>>>(M, P, out->bufs[2], (CntT*)out->bufs[3],
-                                                                      flags);
+        k_pack_fill<int32_t, MODE, CntT><<<blocks, kThreads, 0, st>>>(
+            M, P, out->bufs[2], (CntT*)out->bufs[3], (float*)out->bufs[4], flags);
       else
-        k_pack_fill<int64_t, MODE, CntT><<<blocks, kThreads, 0, st>>>(M, P, out->bufs[2], (CntT*)out->bufs[3],
-                                                                      flags);
+        k_pack_fill<int64_t, MODE, CntT><<<blocks, kThreads, 0, st>>>(
+            M, P, out->bufs[2], (CntT*)out->bufs[3], (float*)out->bufs[4], flags);
       return cudaGetLastError();
     });
     if (e != cudaSuccess) return cleanup(), e;
@@ -951,8 +1035,27 @@ cudaError_t build_pack(const ViModel& M, int64_t nc, int g, int del, PackStore* 
 cudaError_t launch_vi_chunks(const ViPack& P, int64_t c_begin, int64_t c_end, const float* Vin,
                              float* Vout, int32_t* pi, unsigned long long* resid, cudaStream_t st,
                              int tune, unsigned int* err) {
-  (void)err;
   if (c_end <= c_begin) return cudaSuccess;
+  if ((tune & VI_TUNE_TMA) && P.ent_mode == ENT_PACKED && err && P.na <= 32) {
+    // staging shape: chunks per super-chunk, stages, entry bytes per stage
+    auto run = [&](auto kern, int sc_chunks, int bytes) -> cudaError_t {
+      cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+      if (e != cudaSuccess) return e;
+      int per_sm = 0;
+      e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kThreads, bytes);
+      if (e != cudaSuccess) return e;
+      const int64_t n_sc = (c_end - c_begin + sc_chunks - 1) / sc_chunks;
+      const int64_t cap = (int64_t)std::max(per_sm, 1) * sm_count_pack();
+      const unsigned grid = (unsigned)std::min(n_sc, cap);
+      kern<<<grid, kThreads, bytes, st>>>(P, (int)c_begin, (int)c_end, Vin, Vout, pi, resid, err);
+      return cudaGetLastError();
+    };
+    // measured on c2: 2 chunks x 2 stages 2.0 TB/s; 4 stages (1 CTA/SM) 1.0,
+    // 4 chunks x 3 stages 1.4, 1 chunk x 4 stages 1.3; the register-streaming
+    // lean sweep 3.9: with 8-16 resident warps the V-gather chains, not DRAM
+    // latency, bound the staged sweep
+    return run(k_vi_tma<2, 2, 40 * 1024>, 2, 2 * sc_stage_bytes<2, 40 * 1024>(P.na, P.na_pad));
+  }
   const int prefetch = tune & (PF_NEXT | PF_CURRENT);
   return dispatch_pack(P, [&](auto mode, auto* cntt) -> cudaError_t {
     using CntT = std::remove_pointer_t<decltype(cntt)>;
@@ -970,7 +1073,6 @@ cudaError_t launch_vi_chunks(const ViPack& P, int64_t c_begin, int64_t c_end, co
 cudaError_t launch_vi_layered(const ViPack& P, float* V, int32_t* pi, unsigned int* sync, int groups,
                               cudaStream_t st, int tune) {
   const int prefetch = tune & (PF_NEXT | PF_CURRENT);
-  const int nsl = (int)std::min<int64_t>(kSlices, ((int64_t)P.gs * P.na + 31) / 32);
   return dispatch_pack(P, [&](auto mode, auto* cntt) -> cudaError_t {
     using CntT = std::remove_pointer_t<decltype(cntt)>;
     constexpr int MODE = decltype(mode)::value;
@@ -979,9 +1081,9 @@ cudaError_t launch_vi_layered(const ViPack& P, float* V, int32_t* pi, unsigned i
     const int64_t cap = (int64_t)occupancy((const void*)kern) * sm_count_pack();
     int G = groups;
     if (G <= 0) {
-      // enough warps for one layer's groups: split slices while that adds warps
+      // enough warps for one layer's chunks: split actions while that adds warps
       G = 1;
-      while (G < 8 && G * 2 <= nsl && P.cpl * G * 2 <= cap * kWarps) G *= 2;
+      while (G < 8 && G * 2 <= P.na && P.cpl * G * 2 <= cap * kWarps) G *= 2;
     }
     if (G != 1 && G != 2 && G != 4 && G != 8) return cudaErrorInvalidValue;
     const int cpc = kWarps / G;
