@@ -228,10 +228,15 @@ e2e_status solve_batch(const std::vector<BatchJobSpec>& jobs, int schedule, cuda
       H->njobs = n;
       H->max_layers = maxL;
       const int mode = kv.first.first, cnt = kv.first.second;
+      // CTAs: enough for the widest step, rounded up to a power of two so that
+      // batches of similar size share one captured graph (a new launch shape
+      // costs a capture and an instantiation; surplus CTAs find no items)
       auto grid_for = [&](const Choice& c) {
         const int cap = vi_batch_capacity(mode, cnt, c.tune);
         const int64_t need = (total + (8 / c.groups) - 1) / (8 / c.groups);
-        return (int)std::max<int64_t>(1, std::min<int64_t>(cap, need));
+        int64_t q = 1;
+        while (q < need) q <<= 1;
+        return (int)std::max<int64_t>(1, std::min<int64_t>(cap, q));
       };
       Choice ch;
       if (tune_given) {

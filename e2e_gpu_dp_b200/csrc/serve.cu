@@ -136,6 +136,9 @@ struct Req {
 
 }  // namespace
 
+// models above this many states are solved in launches of their own
+constexpr int64_t kLargeStates = 4000000;
+
 struct Server {
   e2e_server_opts opts{};
   int device = 0;
@@ -398,7 +401,11 @@ struct Server {
         jobs.push_back(js);
         run.push_back(q);
       }
-      if (!run.empty()) {
+      // one launch per group: requests on large models (more than
+      // kLargeStates states) after the others, so that a batch of small
+      // requests never waits for a large model's solve in the same launch
+      auto run_group = [&](std::vector<BatchJobSpec>& jobs, std::vector<Req*>& run) {
+        if (run.empty()) return;
         BatchResult br;
         // the heuristic schedule unless one is given: no timing runs in the request path
         e2e_status s = solve_batch(jobs, opts.schedule ? opts.schedule : 0x400, st, &br);
@@ -433,7 +440,26 @@ struct Server {
           }
           finish(q, s);
         }
+      };
+      std::vector<BatchJobSpec> jobs_large;
+      std::vector<Req*> run_large;
+      {
+        size_t w = 0;
+        for (size_t k = 0; k < run.size(); ++k) {
+          if (jobs[k].m->ns > kLargeStates) {
+            jobs_large.push_back(jobs[k]);
+            run_large.push_back(run[k]);
+          } else {
+            jobs[w] = jobs[k];
+            run[w] = run[k];
+            ++w;
+          }
+        }
+        jobs.resize(w);
+        run.resize(w);
       }
+      run_group(jobs, run);
+      run_group(jobs_large, run_large);
       if (!later.empty()) {
         std::lock_guard<std::mutex> lk(mu);
         for (auto it = later.rbegin(); it != later.rend(); ++it) pending.push_front(*it);
