@@ -106,13 +106,13 @@ struct ViPack {
   int64_t ns, nc;          // states; states per layer (ns when the model has no layers)
   int64_t cpl, nchunks;    // chunks of 32 states per layer; all chunks
   int64_t n_row_states;    // states that own rows
-  int64_t slot_rows;       // slot rows of 16 entries (one chunk half)
+  int64_t slot_rows;       // slot rows of 32 entries
   int nlayers, na, na_pad, nrzns, count_type, ent_mode;
   int g, del;              // grid side and window half-width (window-offset column base)
-  const int64_t* chunk_slot;  // 2 * nchunks + 1: first slot row of each chunk half
-  const uint16_t* maxlen;     // 2 * nchunks * na_pad: slot rows per (chunk, half, action)
-  const void* col;            // slot_rows * 16: packed entries, uint16 offsets or int32 columns
-  const void* cnt;            // slot_rows * 16: counts / values (null for ENT_PACKED)
+  const int64_t* chunk_slot;  // nchunks + 1: first slot row of each chunk
+  const uint16_t* maxlen;     // nchunks * na_pad: slot rows per (chunk, action)
+  const void* col;            // slot_rows * 32: packed entries, uint16 offsets or int32 columns
+  const void* cnt;            // slot_rows * 32: counts / values (null for ENT_PACKED)
   const float* R;             // nchunks * na * 32: [chunk][action][lane]
 };
 
@@ -131,11 +131,11 @@ void free_pack(PackStore* p);
 int64_t pack_sweep_bytes(const ViPack& P);
 // tune bits of the sweeps: L2 bulk prefetch of the chunk a warp takes next
 // (the next layer's, when layered) and/or of the chunk it starts; the lean
-// kernel (no entry look-ahead, 8 CTAs per SM) instead of the look-ahead one.
-// Bit 3 is accepted and has no effect.
-enum : int { VI_TUNE_PF_NEXT = 1, VI_TUNE_PF_CURRENT = 2, VI_TUNE_LEAN = 4 };
+// kernel (no entry look-ahead, 8 CTAs per SM) instead of the look-ahead one;
+// for the Jacobi sweep of the packed layout, the TMA-staged kernel
+enum : int { VI_TUNE_PF_NEXT = 1, VI_TUNE_PF_CURRENT = 2, VI_TUNE_LEAN = 4, VI_TUNE_TMA = 8 };
 // One Jacobi sweep over chunks [c_begin, c_end).
-// err: unused (kept for callers that pass their error word)
+// err: device word for bounded-wait failures (needed by the TMA-staged kernel)
 cudaError_t launch_vi_chunks(const ViPack& P, int64_t c_begin, int64_t c_end, const float* Vin,
                              float* Vout, int32_t* pi, unsigned long long* resid, cudaStream_t st,
                              int tune, unsigned int* err = nullptr);

@@ -3,15 +3,12 @@
 //
 // Layout.  States are taken in chunks of 32 consecutive states of one layer
 // (a chunk never crosses a layer boundary; the last chunk of a layer is
-// partial).  Lane l of a warp owns state l of a chunk.  Each half of a chunk
-// (lanes 0-15, 16-31) stores, for action a, maxlen[c][h][a] "slot rows" of 16
-// entries; entry k of row (s, a) sits at
-//   slot (chunk_slot[2c + h] + sum_{b<a} maxlen[c][h][b] + k) * 16 + (lane(s) & 15)
-// so the k-th entries of a half's 16 rows (s, a) are one coalesced 64-byte
-// segment.  Rows shorter than their half's maxlen are padded with count 0;
-// padding to the longer of 16 rows instead of 32 cuts it from 33.7 % to 21.9 %
-// of the entries on the 200x200x120 model.  R is stored beside it as
-// [chunk][action][lane].
+// partial).  Lane l of a warp owns state l of a chunk.  For action a, a chunk
+// stores maxlen[c][a] "slot rows" of 32 entries; entry k of row (s, a) sits at
+//   slot (chunk_slot[c] + sum_{b<a} maxlen[c][b] + k) * 32 + lane(s)
+// so the k-th entries of the 32 rows (s, a) of a chunk are one coalesced
+// 128-byte line.  Rows shorter than maxlen are padded with count 0.  R is
+// stored beside it as [chunk][action][lane].
 //
 // Columns: on a time-layered model built on a g x g grid, every next state of
 // a layer-t cell (i, j) lies in layer t+1 inside the m x m window centred on
@@ -47,7 +44,6 @@ namespace {
 
 constexpr int kThreads = 256;
 constexpr int kWarps = kThreads / 32;
-constexpr int kHalf = 16;  // entries per slot row: one half of a chunk
 constexpr int PF_NEXT = VI_TUNE_PF_NEXT;
 constexpr int PF_CURRENT = VI_TUNE_PF_CURRENT;
 constexpr long long kBarrierSpinLimit = 1ll << 22;
@@ -151,8 +147,8 @@ struct Entries {
   const ColT* col;
   const CntT* cnt;
   __device__ __forceinline__ void advance(int rows) {
-    col += rows * kHalf;
-    if (MODE != ENT_PACKED) cnt += rows * kHalf;
+    col += rows * 32;
+    if (MODE != ENT_PACKED) cnt += rows * 32;
   }
   // this lane's first n (<= B) entries, zeros beyond; a full batch loads unpredicated
   template <int B>
@@ -160,8 +156,8 @@ struct Entries {
     if (n == B) {
 #pragma unroll
       for (int j = 0; j < B; ++j) {
-        o[j] = ld_stream(col + j * kHalf);
-        w[j] = MODE != ENT_PACKED ? ld_stream(cnt + j * kHalf) : (CntT)0;
+        o[j] = ld_stream(col + j * 32);
+        w[j] = MODE != ENT_PACKED ? ld_stream(cnt + j * 32) : (CntT)0;
       }
       return;
     }
@@ -170,8 +166,8 @@ struct Entries {
       o[j] = 0;
       w[j] = 0;
       if (j < n) {
-        o[j] = ld_stream(col + j * kHalf);
-        if (MODE != ENT_PACKED) w[j] = ld_stream(cnt + j * kHalf);
+        o[j] = ld_stream(col + j * 32);
+        if (MODE != ENT_PACKED) w[j] = ld_stream(cnt + j * 32);
       }
     }
   }
@@ -201,13 +197,11 @@ __device__ __forceinline__ void chunk_best(const ViPack& P, int c, const ChunkPo
   using E = Entries<MODE, CntT>;
   using ColT = typename E::ColT;
   constexpr int B = 4;
-  const int h = lane >> 4;  // the lane's half of the chunk: its own slot rows and lengths
-  const uint16_t* mlp = P.maxlen + ((int64_t)c * 2 + h) * P.na_pad;
-  int64_t slot = __ldg(P.chunk_slot + 2 * c + h);
+  const uint16_t* mlp = P.maxlen + (int64_t)c * P.na_pad;
+  int64_t slot = __ldg(P.chunk_slot + c);
   for (int b = 0; b < a0; ++b) slot += __ldg(mlp + b);
-  const int64_t e0 = slot * kHalf + (lane & (kHalf - 1));
-  E cur{reinterpret_cast<const ColT*>(P.col) + e0,
-        MODE == ENT_PACKED ? nullptr : reinterpret_cast<const CntT*>(P.cnt) + e0};
+  E cur{reinterpret_cast<const ColT*>(P.col) + slot * 32 + lane,
+        MODE == ENT_PACKED ? nullptr : reinterpret_cast<const CntT*>(P.cnt) + slot * 32 + lane};
   const float* vb = MODE == ENT_I32 ? Vin : Vin + cp.base;
   const bool counts = P.count_type != VAL_F32;
   auto fold = [&](const ColT(&o)[B], const CntT(&w)[B], int n, float& acc) {
@@ -285,12 +279,12 @@ struct Widths {
 
 // L2 prefetch of chunk c: entry streams and R (bulk prefetch, one lane)
 __device__ __forceinline__ void prefetch_chunk(const ViPack& P, int c, int col_bytes, int cnt_bytes) {
-  const int64_t s0 = __ldg(P.chunk_slot + 2 * c), s1 = __ldg(P.chunk_slot + 2 * c + 2);
-  const int64_t n = (s1 - s0) * kHalf;
+  const int64_t s0 = __ldg(P.chunk_slot + c), s1 = __ldg(P.chunk_slot + c + 1);
+  const int64_t n = (s1 - s0) * 32;
   if (n > 0) {
-    prefetch_l2(reinterpret_cast<const char*>(P.col) + s0 * kHalf * col_bytes, (uint32_t)(n * col_bytes));
+    prefetch_l2(reinterpret_cast<const char*>(P.col) + s0 * 32 * col_bytes, (uint32_t)(n * col_bytes));
     if (cnt_bytes)
-      prefetch_l2(reinterpret_cast<const char*>(P.cnt) + s0 * kHalf * cnt_bytes, (uint32_t)(n * cnt_bytes));
+      prefetch_l2(reinterpret_cast<const char*>(P.cnt) + s0 * 32 * cnt_bytes, (uint32_t)(n * cnt_bytes));
   }
   prefetch_l2(P.R + (int64_t)c * P.na * 32, (uint32_t)(P.na * 32 * 4));
 }
@@ -338,6 +332,215 @@ __global__ void __launch_bounds__(kThreads, MinBlocks<MODE, VAR>::value)
     if (lane == 0) wmax[threadIdx.x >> 5] = dmax;
     __syncthreads();
     if (threadIdx.x == 0) {
+      double mx = 0.0;
+      for (int w = 0; w < kWarps; ++w) mx = fmax(mx, wmax[w]);
+      if (mx > 0.0) atomicMax(resid, (unsigned long long)__double_as_longlong(mx));
+    }
+  }
+}
+
+// ---- TMA-staged Jacobi sweep (packed layout) ---------------------------------------
+// A CTA walks super-chunks of SC consecutive chunks; their entries, R and
+// per-action lengths are contiguous ranges of the sliced copy, so one thread
+// stages super-chunks NST-1 ahead with three 1-D bulk copies each
+// (cp.async.bulk, completion counted on an mbarrier per stage) into a ring of
+// NST shared-memory stages while the CTA computes: 8/SC warps per chunk,
+// each a block of actions, reading entries from shared memory
+// (conflict-free: lane l reads word l of a slot row) and gathering V through
+// L1.  DRAM latency is covered by the double buffer instead of by resident
+// warps.  A super-chunk whose entries exceed a stage is read from global
+// memory.  Waits are bounded (error bit 8 of err).
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return (uint32_t)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// 1-D bulk copy global -> this CTA's shared memory (no multicast); 16-byte
+// aligned addresses, size a multiple of 16
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+          smem_u32(dst)),
+      "l"(src), "r"(bytes), "r"(smem_u32(bar))
+      : "memory");
+}
+__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+__device__ __forceinline__ void fence_mbar_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
+
+template <int SC>
+__host__ __device__ __forceinline__ int sc_r_bytes(int na) { return SC * na * 32 * 4; }
+template <int SC>
+__host__ __device__ __forceinline__ int sc_ml_bytes(int na_pad) { return (SC * na_pad * 2 + 15) & ~15; }
+template <int SC, int EB>
+__host__ __device__ __forceinline__ int sc_stage_bytes(int na, int na_pad) {
+  return EB + sc_r_bytes<SC>(na) + sc_ml_bytes<SC>(na_pad);
+}
+
+template <int SC, int NST, int EB>
+__global__ void __launch_bounds__(kThreads)
+    k_vi_tma(ViPack P, int c_begin, int c_end, const float* __restrict__ Vin, float* Vout, int32_t* pi,
+             unsigned long long* resid, unsigned int* err) {
+  constexpr int kScChunks = SC;
+  constexpr int kScG = kWarps / SC;
+  constexpr int kScEntBytes = EB;
+  extern __shared__ __align__(128) unsigned char smem[];
+  __shared__ uint64_t bar[NST];
+  __shared__ int s_ok, s_direct[NST];
+  __shared__ float sq[kWarps][32];
+  __shared__ int sa[kWarps][32];
+  __shared__ double wmax[kWarps];
+  const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+  const int na = P.na, na_pad = P.na_pad;
+  const int stage_bytes = sc_stage_bytes<SC, EB>(na, na_pad);
+  const int n_sc = (c_end - c_begin + kScChunks - 1) / kScChunks;
+  const int cc = wid / kScG, grp = wid % kScG;
+  const int apg = (na + kScG - 1) / kScG;
+  const int a0 = min(na, grp * apg), a1 = min(na, a0 + apg);
+  const bool counts = P.count_type != VAL_F32;
+
+  auto issue = [&](int sc, int st) {  // thread 0
+    const int c0 = c_begin + sc * kScChunks, c1 = min(c0 + kScChunks, c_end);
+    const int64_t e0 = __ldg(P.chunk_slot + c0), e1 = __ldg(P.chunk_slot + c1);
+    const int64_t eb = (e1 - e0) * 128;
+    unsigned char* sp = smem + st * stage_bytes;
+    if (eb > kScEntBytes) {  // too large for a stage: read from global memory
+      s_direct[st] = 1;
+      mbar_expect_tx(&bar[st], 0);
+      return;
+    }
+    s_direct[st] = 0;
+    const uint32_t rb = (uint32_t)((c1 - c0) * na * 128);
+    const uint32_t mb = (uint32_t)((c1 - c0) * na_pad * 2);
+    mbar_expect_tx(&bar[st], (uint32_t)eb + rb + mb);
+    if (eb) bulk_g2s(sp, reinterpret_cast<const char*>(P.col) + e0 * 128, (uint32_t)eb, &bar[st]);
+    bulk_g2s(sp + kScEntBytes, P.R + (int64_t)c0 * na * 32, rb, &bar[st]);
+    bulk_g2s(sp + kScEntBytes + sc_r_bytes<SC>(na), P.maxlen + (int64_t)c0 * na_pad, mb, &bar[st]);
+  };
+
+  if (tid == 0) {
+    for (int q = 0; q < NST; ++q) mbar_init(&bar[q], 1);
+    fence_mbar_init();
+  }
+  __syncthreads();
+  int sc = blockIdx.x;
+  if (tid == 0)
+    for (int q = 0; q < NST - 1; ++q)
+      if (sc + q * (int)gridDim.x < n_sc) issue(sc + q * gridDim.x, q);
+  double dmax = 0.0;
+  bool failed = false;
+  for (int k = 0; sc < n_sc; ++k, sc += gridDim.x) {
+    const int st = k % NST;
+    if (tid == 0) {
+      const int ahead = sc + (NST - 1) * (int)gridDim.x;
+      if (ahead < n_sc) {
+        fence_proxy_async();  // that stage was read through the generic proxy
+        issue(ahead, (k + NST - 1) % NST);
+      }
+      long long it = 0;
+      const uint32_t parity = (uint32_t)((k / NST) & 1);
+      while (!mbar_try_wait(&bar[st], parity) && ++it < (1ll << 24)) {
+      }
+      s_ok = it < (1ll << 24);
+    }
+    __syncthreads();
+    if (!s_ok) {
+      if (tid == 0) atomicOr(err, 8u);
+      failed = true;
+      break;
+    }
+    const int c0 = c_begin + sc * kScChunks;
+    const int c = c0 + cc;
+    const bool active = c < c_end;
+    float bq = -INFINITY;
+    int ba = 0x7fffffff;
+    ChunkPos cp{0, 0, false};
+    if (active) {
+      cp = chunk_pos(P, c, lane, true);
+      if (s_direct[st]) {
+        chunk_best<ENT_PACKED, uint16_t, false, 1>(P, c, cp, lane, a0, a1, Vin, bq, ba, pack_r(P, c, a0, lane), 32);
+      } else {
+        const unsigned char* sp = smem + st * stage_bytes;
+        const uint32_t* ent = reinterpret_cast<const uint32_t*>(sp);
+        const float* Rs = reinterpret_cast<const float*>(sp + kScEntBytes);
+        const uint16_t* mls = reinterpret_cast<const uint16_t*>(sp + kScEntBytes + sc_r_bytes<SC>(na)) + cc * na_pad;
+        int64_t slot = __ldg(P.chunk_slot + c) - __ldg(P.chunk_slot + c0);
+        for (int b = 0; b < a0; ++b) slot += mls[b];
+        const uint32_t* ep = ent + slot * 32 + lane;
+        const float* rp = Rs + ((int64_t)cc * na + a0) * 32 + lane;
+        const float* vb = Vin + cp.base;
+        for (int a = a0; a < a1; ++a) {
+          const int ml = mls[a];
+          float acc = 0.f;
+          for (int k0 = 0; k0 < ml; k0 += 4) {
+            const int n = min(ml - k0, 4);
+            uint32_t e[4];
+            float v[4];
+#pragma unroll
+            for (int j = 0; j < 4; ++j) e[j] = j < n ? ep[(k0 + j) * 32] : 0u;
+#pragma unroll
+            for (int j = 0; j < 4; ++j) v[j] = j < n ? __ldg(vb + (e[j] & 0xffffu)) : 0.f;
+#pragma unroll
+            for (int j = 0; j < 4; ++j) acc = fmaf((float)(e[j] >> 16), v[j], acc);  // padding: exact no-op
+          }
+          ep += ml * 32;
+          const float q = finish_row(*rp, acc, 0.f, P.nrzns, counts);
+          rp += 32;
+          if (!isnan(q) && q > bq) {
+            bq = q;
+            ba = a;
+          }
+        }
+      }
+    }
+    sq[wid][lane] = bq;
+    sa[wid][lane] = ba;
+    __syncthreads();  // candidates in place; the stage is consumed
+    if (active && grp == 0) {
+      for (int g2 = 1; g2 < kScG; ++g2) {
+        const float oq = sq[wid + g2][lane];
+        if (oq > bq) {  // later groups hold later actions: strict '>' keeps the first maximum
+          bq = oq;
+          ba = sa[wid + g2][lane];
+        }
+      }
+      if (cp.valid) {
+        float vout;
+        int32_t pout;
+        finish_state(bq, ba, vout, pout);
+        if (resid) dmax = fmax(dmax, fabs((double)vout - (double)Vin[cp.s]));
+        Vout[cp.s] = vout;
+        pi[cp.s] = pout;
+      }
+    }
+    __syncthreads();  // sq/sa free for the next super-chunk
+  }
+  if (failed && tid == 0) {
+    // give the copies in flight time to land before the CTA exits
+    for (int st = 0; st < NST; ++st) {
+      long long it = 0;
+      while (!mbar_try_wait(&bar[st], 0) && !mbar_try_wait(&bar[st], 1) && ++it < (1ll << 24)) {
+      }
+    }
+  }
+  if (resid) {
+    for (int off = 16; off > 0; off >>= 1) dmax = fmax(dmax, __shfl_xor_sync(0xffffffffu, dmax, off));
+    if (lane == 0) wmax[wid] = dmax;
+    __syncthreads();
+    if (tid == 0) {
       double mx = 0.0;
       for (int w = 0; w < kWarps; ++w) mx = fmax(mx, wmax[w]);
       if (mx > 0.0) atomicMax(resid, (unsigned long long)__double_as_longlong(mx));
@@ -589,11 +792,11 @@ __global__ void __launch_bounds__(kThreads, BatchMinBlocks<MODE, VAR>::value)
 
 // ---- pack construction ------------------------------------------------------------
 
-// per chunk half: maxlen of every action over the half's 16 rows, and their sum
+// per chunk: maxlen of every action over the chunk's 32 rows, and their sum
 template <typename PtrT>
 __global__ void __launch_bounds__(kThreads) k_pack_count(ViModel M, ViPack P, int32_t* slot_len,
                                                          uint16_t* maxlen) {
-  const int lane = threadIdx.x & 31, h = lane >> 4;
+  const int lane = threadIdx.x & 31;
   const int c = blockIdx.x * kWarps + (threadIdx.x >> 5);
   if (c >= P.nchunks) return;
   const ChunkPos cp = chunk_pos(P, c, lane, false);
@@ -601,7 +804,6 @@ __global__ void __launch_bounds__(kThreads) k_pack_count(ViModel M, ViPack P, in
   const PtrT* rp = reinterpret_cast<const PtrT*>(M.row_ptr);
   int64_t prev = has ? (int64_t)rp[cp.s * P.na] : 0;
   int total = 0;
-  uint16_t* mlh = maxlen + ((int64_t)c * 2 + h) * P.na_pad;
   for (int a = 0; a < P.na; ++a) {
     unsigned len = 0;
     if (has) {
@@ -609,15 +811,13 @@ __global__ void __launch_bounds__(kThreads) k_pack_count(ViModel M, ViPack P, in
       len = (unsigned)(nx - prev);
       prev = nx;
     }
-    unsigned ml = len;  // maximum over the 16 lanes of this half
-#pragma unroll
-    for (int o = 8; o > 0; o >>= 1) ml = max(ml, __shfl_xor_sync(0xffffffffu, ml, o));
-    if ((lane & 15) == 0) mlh[a] = (uint16_t)ml;
+    const unsigned ml = __reduce_max_sync(0xffffffffu, len);
+    if (lane == 0) maxlen[(int64_t)c * P.na_pad + a] = (uint16_t)ml;
     total += (int)ml;
   }
-  if ((lane & 15) == 0) {
-    for (int a = P.na; a < P.na_pad; ++a) mlh[a] = 0;
-    slot_len[2 * c + h] = total;
+  if (lane == 0) {
+    for (int a = P.na; a < P.na_pad; ++a) maxlen[(int64_t)c * P.na_pad + a] = 0;
+    slot_len[c] = total;
   }
 }
 
@@ -633,20 +833,19 @@ __global__ void __launch_bounds__(kThreads) k_pack_fill(ViModel M, ViPack P, voi
   const bool has = cp.valid && cp.s < P.n_row_states;
   const PtrT* rp = reinterpret_cast<const PtrT*>(M.row_ptr);
   const CntT* src = reinterpret_cast<const CntT*>(M.cnt);
-  const int h = lane >> 4;
-  int64_t slot = P.chunk_slot[2 * c + h];
+  int64_t slot = P.chunk_slot[c];
   bool bad = false;
   // lanes without rows gather nothing that is kept; give them a valid index too
   const int32_t pad_col = !has ? 0 : (int32_t)(cp.s / P.nc + 1 < P.nlayers ? cp.s + P.nc : cp.s);
   for (int a = 0; a < P.na; ++a) {
-    const int ml = P.maxlen[((int64_t)c * 2 + h) * P.na_pad + a];
+    const int ml = P.maxlen[(int64_t)c * P.na_pad + a];
     int64_t rs = 0, len = 0;
     if (has) {
       rs = (int64_t)rp[cp.s * P.na + a];
       len = (int64_t)rp[cp.s * P.na + a + 1] - rs;
     }
     for (int k = 0; k < ml; ++k) {
-      const int64_t e = (slot + k) * kHalf + (lane & (kHalf - 1));
+      const int64_t e = (slot + k) * 32 + lane;
       // padding (count 0) points at the lane's own cell in layer t+1, finished
       // before layer t in every schedule, so the gathered value is finite and
       // fma(0, v, acc) leaves acc unchanged
@@ -733,8 +932,8 @@ void free_pack(PackStore* p) {
 
 int64_t pack_sweep_bytes(const ViPack& P) {
   // entries (with padding) + R + chunk tables + V read + V' and policy written
-  return P.slot_rows * kHalf * (col_bytes_of(P) + cnt_bytes_of(P)) + P.nchunks * P.na * 32 * 4 +
-         P.nchunks * 2 * (8 + P.na_pad * 2) + P.ns * 12;
+  return P.slot_rows * 32 * (col_bytes_of(P) + cnt_bytes_of(P)) + P.nchunks * P.na * 32 * 4 +
+         P.nchunks * (8 + P.na_pad * 2) + P.ns * 12;
 }
 
 cudaError_t build_pack(const ViModel& M, int64_t nc, int g, int del, PackStore* out, cudaStream_t st) {
@@ -767,11 +966,10 @@ cudaError_t build_pack(const ViModel& M, int64_t nc, int g, int del, PackStore* 
     dfree(block_sums, st);
     dfree(flags, st);
   };
-  const int64_t nhalves = 2 * P.nchunks;
-  const int64_t nb = (nhalves + 1023) / 1024 + 1;
-  if ((e = dalloc(&out->bufs[0], sizeof(int64_t) * (nhalves + 1), st)) != cudaSuccess) return e;
-  if ((e = dalloc(&out->bufs[1], sizeof(uint16_t) * nhalves * P.na_pad, st)) != cudaSuccess) return e;
-  if ((e = dalloc((void**)&slot_len, sizeof(int32_t) * nhalves, st)) != cudaSuccess) return cleanup(), e;
+  const int64_t nb = (P.nchunks + 1023) / 1024 + 1;
+  if ((e = dalloc(&out->bufs[0], sizeof(int64_t) * (P.nchunks + 1), st)) != cudaSuccess) return e;
+  if ((e = dalloc(&out->bufs[1], sizeof(uint16_t) * P.nchunks * P.na_pad, st)) != cudaSuccess) return e;
+  if ((e = dalloc((void**)&slot_len, sizeof(int32_t) * P.nchunks, st)) != cudaSuccess) return cleanup(), e;
   if ((e = dalloc((void**)&block_sums, sizeof(int64_t) * nb, st)) != cudaSuccess) return cleanup(), e;
   if ((e = dalloc((void**)&flags, sizeof(unsigned int) * 2, st)) != cudaSuccess) return cleanup(), e;
   P.chunk_slot = (const int64_t*)out->bufs[0];
@@ -783,10 +981,10 @@ cudaError_t build_pack(const ViModel& M, int64_t nc, int g, int del, PackStore* 
     k_pack_count<int64_t><<<blocks, kThreads, 0, st>>>(M, P, slot_len, (uint16_t*)out->bufs[1]);
   if ((e = cudaGetLastError()) != cudaSuccess) return cleanup(), e;
   int64_t* cs = (int64_t*)out->bufs[0];
-  if ((e = launch_scan_tiles(slot_len, nhalves, cs, cs + nhalves, block_sums, st)) != cudaSuccess)
+  if ((e = launch_scan_tiles(slot_len, P.nchunks, cs, cs + P.nchunks, block_sums, st)) != cudaSuccess)
     return cleanup(), e;
   int64_t slot_rows = 0;
-  if ((e = cudaMemcpyAsync(&slot_rows, cs + nhalves, sizeof(int64_t), cudaMemcpyDeviceToHost, st)) !=
+  if ((e = cudaMemcpyAsync(&slot_rows, cs + P.nchunks, sizeof(int64_t), cudaMemcpyDeviceToHost, st)) !=
       cudaSuccess)
     return cleanup(), e;
   if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return cleanup(), e;
@@ -797,9 +995,9 @@ cudaError_t build_pack(const ViModel& M, int64_t nc, int g, int del, PackStore* 
   for (int attempt = 0; attempt < 2; ++attempt) {
     const int cb = col_bytes_of(P), nb2 = cnt_bytes_of(P);
     // 16 spare elements keep every bulk prefetch inside its allocation
-    if ((e = dalloc(&out->bufs[2], (size_t)(slot_rows * kHalf + 16) * cb, st)) != cudaSuccess)
+    if ((e = dalloc(&out->bufs[2], (size_t)(slot_rows * 32 + 16) * cb, st)) != cudaSuccess)
       return cleanup(), e;
-    if (nb2 && (e = dalloc(&out->bufs[3], (size_t)(slot_rows * kHalf + 16) * nb2, st)) != cudaSuccess)
+    if (nb2 && (e = dalloc(&out->bufs[3], (size_t)(slot_rows * 32 + 16) * nb2, st)) != cudaSuccess)
       return cleanup(), e;
     P.col = out->bufs[2];
     P.cnt = out->bufs[3];
@@ -838,7 +1036,26 @@ cudaError_t launch_vi_chunks(const ViPack& P, int64_t c_begin, int64_t c_end, co
                              float* Vout, int32_t* pi, unsigned long long* resid, cudaStream_t st,
                              int tune, unsigned int* err) {
   if (c_end <= c_begin) return cudaSuccess;
-  (void)err;
+  if ((tune & VI_TUNE_TMA) && P.ent_mode == ENT_PACKED && err && P.na <= 32) {
+    // staging shape: chunks per super-chunk, stages, entry bytes per stage
+    auto run = [&](auto kern, int sc_chunks, int bytes) -> cudaError_t {
+      cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+      if (e != cudaSuccess) return e;
+      int per_sm = 0;
+      e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kThreads, bytes);
+      if (e != cudaSuccess) return e;
+      const int64_t n_sc = (c_end - c_begin + sc_chunks - 1) / sc_chunks;
+      const int64_t cap = (int64_t)std::max(per_sm, 1) * sm_count_pack();
+      const unsigned grid = (unsigned)std::min(n_sc, cap);
+      kern<<<grid, kThreads, bytes, st>>>(P, (int)c_begin, (int)c_end, Vin, Vout, pi, resid, err);
+      return cudaGetLastError();
+    };
+    // measured on c2: 2 chunks x 2 stages 2.0 TB/s; 4 stages (1 CTA/SM) 1.0,
+    // 4 chunks x 3 stages 1.4, 1 chunk x 4 stages 1.3; the register-streaming
+    // lean sweep 3.9: with 8-16 resident warps the V-gather chains, not DRAM
+    // latency, bound the staged sweep
+    return run(k_vi_tma<2, 2, 40 * 1024>, 2, 2 * sc_stage_bytes<2, 40 * 1024>(P.na, P.na_pad));
+  }
   const int prefetch = tune & (PF_NEXT | PF_CURRENT);
   return dispatch_pack(P, [&](auto mode, auto* cntt) -> cudaError_t {
     using CntT = std::remove_pointer_t<decltype(cntt)>;
