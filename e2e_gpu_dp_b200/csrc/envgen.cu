@@ -37,6 +37,7 @@
 #include <math.h>
 
 #include <algorithm>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -326,22 +327,29 @@ __global__ void k_env_cloud(CloudArgs a) {
 // row-major buffer is the column-major ncols x nws matrix X^T, which gesvdj
 // takes directly when ncols >= nws (X^T = U S V^T: X's left vectors are V);
 // otherwise X is transposed into column-major nws x ncols first.
-// cuSOLVER and cuBLAS handles, one pair per host thread and device, kept for
-// the thread's lifetime (never destroyed: a thread-exit destructor could run
-// after the CUDA context is gone).  Creating them on every call allocated
-// their device work space through the driver each time, which on a busy
-// machine added tens of milliseconds to a 35 ms generation.
-e2e_status solver_handles(cusolverDnHandle_t* sol, cublasHandle_t* blas) {
-  struct Pair {
-    cusolverDnHandle_t sol;
-    cublasHandle_t blas;
-  };
-  thread_local Pair h[64] = {};
+// cuSOLVER and cuBLAS handles, one pair per device for the whole process,
+// created on first use and kept until exit (never destroyed: a destructor at
+// process exit could run after the CUDA context is gone).  A call holds the
+// device's mutex while it uses them, so calls from any number of host
+// threads share one pair and one work space; generations on one device run
+// one at a time.  Creating the handles on every call allocated their device
+// work space through the driver each time, which on a busy machine added tens
+// of milliseconds to a 35 ms generation.  The handles belong to the device's
+// primary context: after cudaDeviceReset the process must not generate again.
+struct DevHandles {
+  std::mutex mu;
+  cusolverDnHandle_t sol = nullptr;
+  cublasHandle_t blas = nullptr;
+};
+DevHandles g_handles[64];
+
+e2e_status solver_handles(cusolverDnHandle_t* sol, cublasHandle_t* blas, std::unique_lock<std::mutex>* hold) {
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return cuda_fail(e, "cudaGetDevice");
   if (dev < 0 || dev >= 64) return fail(E2E_ERR_UNSUPPORTED, "device index above 63");
-  Pair& x = h[dev];
+  DevHandles& x = g_handles[dev];
+  std::unique_lock<std::mutex> lk(x.mu);
   if (!x.sol && cusolverDnCreate(&x.sol) != CUSOLVER_STATUS_SUCCESS) {
     x.sol = nullptr;
     return fail(E2E_ERR_CUDA, "cusolverDnCreate");
@@ -352,6 +360,7 @@ e2e_status solver_handles(cusolverDnHandle_t* sol, cublasHandle_t* blas) {
   }
   *sol = x.sol;
   *blas = x.blas;
+  *hold = std::move(lk);
   return E2E_OK;
 }
 
@@ -593,10 +602,17 @@ extern "C" e2e_status e2e_env_generate(const e2e_env_params* p, const int32_t* i
       if (w->params) cusolverDnDestroyGesvdjInfo(w->params);
     }
   } svdfree{&w};
+  std::unique_lock<std::mutex> handles_held;  // the device's handles, until this call returns
   {
-    e2e_status hs = solver_handles(&w.sol, &w.blas);
+    e2e_status hs = solver_handles(&w.sol, &w.blas, &handles_held);
     if (hs != E2E_OK) return hs;
   }
+  // on every return, the work queued with the handles finishes before the
+  // next caller may set them to its own stream
+  struct DrainBeforeRelease {
+    cudaStream_t s;
+    ~DrainBeforeRelease() { cudaStreamSynchronize(s); }
+  } drain{st};
   CKS(cusolverDnSetStream(w.sol, st));
   CKB(cublasSetStream(w.blas, st));
   CKB(cublasSetPointerMode(w.blas, CUBLAS_POINTER_MODE_HOST));
