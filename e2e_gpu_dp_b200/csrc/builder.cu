@@ -51,8 +51,10 @@ __device__ __forceinline__ uint32_t bit_range(int lo, int hi, int w) {
   return lo > hi ? 0u : (((2u << hi) - 1u) & ~((1u << lo) - 1u));
 }
 
-static constexpr int kRcw = 64;                 // realisations per warp-private velocity chunk
-static constexpr int kVelStride = kRcw + 2;     // padded (the cells of a warp hit distinct banks) and even (16-byte pairs)
+// Realisations per warp-private velocity chunk: BuildArgs::rc (128 for unit
+// spacing, whose kernels keep no mask table, 64 otherwise; smaller when shared
+// memory is short).  A cell's velocity row has rc + 2 entries: padded so the
+// two cells of a warp hit distinct banks, even for 16-byte pair loads.
 static constexpr uint32_t kOvrFlag = 0x8000u;   // counter bit 15: bin is obstacle-overridden
 static constexpr uint32_t kCountMask = 0x7FFFu;
 
@@ -206,10 +208,14 @@ __global__ void __launch_bounds__(1024) k_build_tiles(BuildArgs A) {
   const int nm = P.nm;
   const int log2S = counter_log2_stride(nthr);
 
+  const int rc = A.rc, vstride = rc + 2;
   float2* modes = reinterpret_cast<float2*>(smem);                         // nm x 32: (ui, vi)
-  float2* velw = modes + nm * 32;                                          // 32 x kVelStride
-  uint64_t* masks = reinterpret_cast<uint64_t*>(velw + 32 * kVelStride);   // MASK_COUNT x nthr
-  uint16_t* win = reinterpret_cast<uint16_t*>(masks + MASK_COUNT * nthr);  // 65 x S: bins, miss bin
+  float2* velw = modes + nm * 32;                                          // 32 x vstride
+  // per-thread bin classes of the general loop (other spacings only): unit
+  // spacing derives them from the bin's position where needed
+  uint64_t* masks = UNIT ? nullptr : reinterpret_cast<uint64_t*>(velw + 32 * vstride);  // MASK_COUNT x nthr
+  uint16_t* win = UNIT ? reinterpret_cast<uint16_t*>(velw + 32 * vstride)
+                       : reinterpret_cast<uint16_t*>(masks + MASK_COUNT * nthr);        // 65 x S: bins, miss bin
   __shared__ uint32_t obsmap[32][kNbWords];
   __shared__ float tab[32][8];
   uint16_t* const wcol = win + counter_col(warp, lane);
@@ -372,11 +378,13 @@ __global__ void __launch_bounds__(1024) k_build_tiles(BuildArgs A) {
     slow = rad ? bins : (bins & ~inwin);
     for (uint64_t mo = ovr; mo; mo &= mo - 1) wcol[(__ffsll((long long)mo) - 1) << log2S] = (uint16_t)kOvrFlag;
   }
-  masks[MASK_OVR * nthr + tid] = ovr;
-  masks[MASK_INWIN * nthr + tid] = inwin;
-  masks[MASK_EDGE * nthr + tid] = edge;
-  masks[MASK_TERM * nthr + tid] = term;
-  masks[MASK_SLOW * nthr + tid] = slow;
+  if (!UNIT) {
+    masks[MASK_OVR * nthr + tid] = ovr;
+    masks[MASK_INWIN * nthr + tid] = inwin;
+    masks[MASK_EDGE * nthr + tid] = edge;
+    masks[MASK_TERM * nthr + tid] = term;
+    masks[MASK_SLOW * nthr + tid] = slow;
+  }
   // Unit cell spacing: every window row is counted (rewards folded from the
   // counters per bin); a warp whose windows reach the grid's edge ring also
   // counts the clamps of move(), which only samples landing in edge bins can
@@ -387,7 +395,7 @@ __global__ void __launch_bounds__(1024) k_build_tiles(BuildArgs A) {
   uint32_t n_drop = 0, n_misbin = 0;
   uint32_t* dense = nullptr;
   const int mm = P.m * P.m;
-  float2* myvel = velw + cl * kVelStride;   // this lane's cell
+  float2* myvel = velw + cl * vstride;     // this lane's cell
   const int per = 1 << lanes_log2;         // lanes sharing a cell
   // constants of the sample loops, held in registers
   const float xs0 = P.xs0, ysn = P.ysn, axmax = P.axmax, aymax = P.aymax;
@@ -411,24 +419,23 @@ __global__ void __launch_bounds__(1024) k_build_tiles(BuildArgs A) {
   // are not counted by the reference (their rewards are): they are dropped here.
   int n_cl = 0;
   auto fold_window = [&]() {
-    const uint64_t m_edge = masks[MASK_EDGE * nthr + tid];
-    const uint64_t m_term = masks[MASK_TERM * nthr + tid];
-    const uint64_t m_in = masks[MASK_INWIN * nthr + tid];
     for (int wl = 0; wl < kWinBins; ++wl) {
       uint16_t* p = wcol + (wl << log2S);
       const uint32_t w = *p;
       const uint32_t c = w & kCountMask;
       if (!c) continue;
+      // the bin's classes (the masks of the set-up, from its position)
+      const int i2 = wi0 + (wl >> 3), j2 = wj0 + (wl & 7);
+      const bool in_nb = abs(i2 - i1) <= P.del && abs(j2 - j1) <= P.del;
       float r;
       if (w & kOvrFlag) {
         r = r_out;
       } else {
-        const int k = bit64(m_edge, wl) ? 1 : 0;
-        const bool tm = bit64(m_term, wl);
+        const int k = (i2 == 0 || i2 == g - 1 || j2 == 0 || j2 == g - 1) ? 1 : 0;
+        const bool tm = is_terminal(P, i2, j2);
         if (!rad) {
           r = tab[aa][(tm ? 4 : 0) + k];
         } else {
-          const int i2 = wi0 + (wl >> 3), j2 = wj0 + (wl & 7);
           const float rad2 = __ldg(A.F.s + (int64_t)(T + 1) * nc + (int64_t)i2 * g + j2);
           r = k ? r_out : 0.f;
           if (tm) r += P.r_term;
@@ -437,9 +444,8 @@ __global__ void __launch_bounds__(1024) k_build_tiles(BuildArgs A) {
         }
       }
       sumR += (float)c * r;
-      if (!bit64(m_in, wl)) {
+      if (!in_nb) {
         n_drop += c;
-        const int i2 = wi0 + (wl >> 3), j2 = wj0 + (wl & 7);
         if (i2 - i1 + P.del < P.m && j2 - j1 + P.del < P.m) n_misbin += c;
         *p = (uint16_t)(w & kOvrFlag);
       }
@@ -461,8 +467,10 @@ __global__ void __launch_bounds__(1024) k_build_tiles(BuildArgs A) {
     const unsigned li = (unsigned)(i2 - wi0), lj = (unsigned)(j2 - wj0);
     if (mode == MODE_WINDOW && li < (unsigned)W && lj < (unsigned)W) {
       const int b = (int)li * kWin + (int)lj;
-      if (bit64(masks[MASK_OVR * nthr + tid], b)) r = r_out;
-      if (bit64(masks[MASK_INWIN * nthr + tid], b)) {
+      // the counter's flag is the bin's obstacle override; in-neighbourhood
+      // is the bin's distance from S1
+      if (wcol[b << log2S] & kOvrFlag) r = r_out;
+      if (abs(i2 - i1) <= P.del && abs(j2 - j1) <= P.del) {
         wcol[b << log2S] += 1;
       } else {
         n_drop++;
@@ -502,8 +510,8 @@ __global__ void __launch_bounds__(1024) k_build_tiles(BuildArgs A) {
   };
 
   // ---- realisations in warp-private chunks ----------------------------------
-  for (int base = 0; base < P.nrzns; base += kRcw) {
-    const int clen = min(kRcw, P.nrzns - base);
+  for (int base = 0; base < P.nrzns; base += rc) {
+    const int clen = min(rc, P.nrzns - base);
     __syncwarp();  // previous chunk consumed
     // extract_velocity, src/build_model.cu:389-401: mean + sum over modes, both
     // sums as one chain of packed fused multiply-adds in the reference's order
@@ -912,11 +920,10 @@ int build_lanes_log2(int na) {
   return l;
 }
 
-size_t build_smem_bytes(int na, int nm, int rc) {
-  (void)rc;
+size_t build_smem_bytes(int na, int nm, int rc, bool unit) {
   const int nthr = 32 << build_lanes_log2(na);
-  return (size_t)2 * nm * 32 * sizeof(float) + (size_t)32 * kVelStride * sizeof(float2) +
-         (size_t)MASK_COUNT * nthr * sizeof(uint64_t) +
+  return (size_t)2 * nm * 32 * sizeof(float) + (size_t)32 * (rc + 2) * sizeof(float2) +
+         (unit ? 0 : (size_t)MASK_COUNT * nthr * sizeof(uint64_t)) +
          (size_t)(kWinBins + 1) * ((size_t)1 << counter_log2_stride(nthr)) * sizeof(uint16_t);
 }
 
@@ -924,7 +931,7 @@ template <typename CntT, bool UNIT, bool FUSED = false>
 static cudaError_t launch_one(const BuildArgs& A, int n_layers, cudaStream_t st) {
   dim3 grid((unsigned)A.tiles_per_layer, (unsigned)n_layers);
   dim3 block((unsigned)(32u << A.lanes_log2));
-  size_t sm = build_smem_bytes(A.P.na, A.P.nm, A.rc);
+  size_t sm = build_smem_bytes(A.P.na, A.P.nm, A.rc, UNIT);
   {
     // the shared-memory cap only grows: builds on other host threads may be
     // launching this kernel with a larger need at the same time

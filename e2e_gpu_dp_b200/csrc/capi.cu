@@ -683,11 +683,24 @@ e2e_status plan_build(const e2e_problem* p, int count_bits, int64_t stage_hint, 
     pl->etiles_per_layer = pl->tiles_per_layer * nwarps;
     pl->n_tiles = pl->etiles_per_layer * (p->nt - 1);
   }
-  pl->rc = pl->na >= 16 ? 128 : 64;
-  size_t sm = build_smem_bytes(pl->na, p->nmodes, pl->rc);
+  // realisations per velocity chunk: 128 for unit spacing (no mask table)
+  // while two 512-thread CTAs still fit an SM, else 64; halved while the
+  // need exceeds 200 KB
+  bool unit;
+  {  // the test of make_dev_problem (unit_step) on the same ticks
+    std::vector<float> xs, ys;
+    host_ticks(p, xs, ys);
+    unit = std::fabs(xs[1] - xs[0]) == 1.0f && std::fabs(ys[1] - ys[0]) == 1.0f;
+  }
+  pl->rc = unit ? 128 : 64;
+  size_t sm = build_smem_bytes(pl->na, p->nmodes, pl->rc, unit);
+  if (unit && pl->na <= 16 && sm > 112 * 1024) {
+    pl->rc = 64;
+    sm = build_smem_bytes(pl->na, p->nmodes, pl->rc, unit);
+  }
   while (sm > 200 * 1024 && pl->rc > 16) {
     pl->rc /= 2;
-    sm = build_smem_bytes(pl->na, p->nmodes, pl->rc);
+    sm = build_smem_bytes(pl->na, p->nmodes, pl->rc, unit);
   }
   if (sm > 220 * 1024) return fail(E2E_ERR_UNSUPPORTED, "shared memory need too large (nmodes/actions)");
   if (pl->tiles_per_layer > 0x7fffffff || p->nt - 1 > 65535)

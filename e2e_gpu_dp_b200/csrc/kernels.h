@@ -26,7 +26,7 @@ struct BuildArgs {
   DevFields F;
   int t0;               // first layer of this launch (blockIdx.y offset)
   int tiles_per_layer;  // CTAs per layer = ceil(ncells / 32); emission tiles are warps
-  int rc;               // (unused) realisations per chunk
+  int rc;               // realisations per warp-private velocity chunk
   int lanes_log2;       // lanes per cell = 1 << lanes_log2 >= na
   int32_t* stage_col;
   void* stage_cnt;
@@ -58,7 +58,7 @@ struct AssembleArgs {
 };
 
 int build_lanes_log2(int na);
-size_t build_smem_bytes(int na, int nm, int rc);
+size_t build_smem_bytes(int na, int nm, int rc, bool unit);
 cudaError_t launch_build_tiles(const BuildArgs& A, int count_bits, int n_layers, cudaStream_t st);
 // One layer of the fused build+backup (uses A.V, A.pi, A.pool, A.counters;
 // no staging): launched for layers nt-2 down to 0 on one stream.
