@@ -653,8 +653,9 @@ __global__ void __launch_bounds__(kThreads, MinBlocks<MODE, VAR>::value)
 // (src/build_model.cu:523-545), i.e. one entry (the cell at t+1, count
 // nrzns) and R = 0, evaluated here with the same operations as that row.
 template <int MODE, int VAR>
-struct BatchMinBlocks {  // the job lookup needs a few more registers than k_vi_layered
-  static constexpr int value = MODE != ENT_PACKED ? 3 : (VAR == 0 ? 4 : 5);
+struct BatchMinBlocks {  // the job lookup needs a few more registers than k_vi_layered (lean: 6 CTAs
+                        // per SM measured 24.1 ms on the 256-model batch, 5: 24.7, 8: 25.5)
+  static constexpr int value = MODE != ENT_PACKED ? 3 : (VAR == 0 ? 4 : 6);
 };
 
 template <int MODE, typename CntT, int VAR>
