@@ -140,7 +140,9 @@ __device__ __forceinline__ void fused_backup(const BuildArgs& A, int T, int64_t 
 // holds cells_per_warp = 32/P cells (P = next power of two >= Na) and lane
 // (c, a) is the row (cell c, action a), so a warp computes the velocities of
 // its own cells (u + sum_k ui_k*Y_k, reference order) into warp-private
-// shared memory, samples without CTA barriers and emits its own rows.
+// shared memory from the chunk's coefficients (staged once per CTA between two
+// barriers a chunk), samples without further CTA barriers and emits its own
+// rows.
 //
 // Per row the 8x8 window of the grid around the mean-flow landing cell is
 // classified once.  The obstacle override is bit 15 of the bin's 16-bit
@@ -158,19 +160,49 @@ __device__ __forceinline__ void fused_backup(const BuildArgs& A, int T, int64_t 
 // FUSED (one launch per layer, A.t0 = the layer): instead of staging the rows,
 // back them up at once against V of layer t+1 (finished by the previous launch
 // of the stream) and write V, policy of layer t; see fused_backup below.
-// Velocity sums of four realisations (rows y0 + r * ystep, r = 0..3) over NP
-// coefficient pairs: the 4 * NP loads of the coefficients (from L2: a layer's
-// coefficients are shared by every CTA of the layer) are issued before the
-// multiply-adds, so their round trips overlap, and each sum is one chain of
-// packed fused multiply-adds in mode order.
+// Row stride (floats) of the staged coefficients: a lane reads 8-byte pairs
+// of row a + 16r, so an even stride with stride/2 odd (or an odd stride) keeps
+// the 16 rows of a warp's loads on distinct banks.
+__host__ __device__ __forceinline__ int coeff_stride(int nm) {
+  return (nm & 1) ? nm : (((nm >> 1) & 1) ? nm : nm + 2);
+}
+
+// Stages the coefficients of clen realisations (rows of nm floats from src)
+// in shared memory, rows ys floats apart: 4-byte asynchronous copies, the
+// CTA's threads striding over the elements; one commit group per call.
+__device__ __forceinline__ void stage_coeffs(float* ysm, int ys, const float* src, int clen, int nm, int tid,
+                                             int nthr) {
+  const int n = clen * nm;
+  int q = tid / nm, k = tid - q * nm;
+  const int dq = nthr / nm, dk = nthr - dq * nm;  // dk < nm
+  for (int idx = tid; idx < n; idx += nthr) {
+    const uint32_t dst = (uint32_t)__cvta_generic_to_shared(ysm + q * ys + k);
+    asm volatile(
+        "{\n\t.reg .u64 g;\n\tcvta.to.global.u64 g, %1;\n\tcp.async.ca.shared.global [%0], [g], 4;\n\t}" ::"r"(dst),
+        "l"(src + idx)
+        : "memory");
+    q += dq;
+    k += dk;
+    if (k >= nm) {
+      k -= nm;
+      ++q;
+    }
+  }
+  asm volatile("cp.async.commit_group;" ::: "memory");
+}
+
+// Velocity sums of four realisations (staged rows y0 + r * ystep, r = 0..3)
+// over NP coefficient pairs: the 4 * NP shared-memory loads are issued before
+// the multiply-adds, and each sum is one chain of packed fused multiply-adds in
+// mode order.
 template <int NP>
-__device__ __forceinline__ void vel_pairs4(const float2* md, const float* y0, int64_t ystep, float2& s0,
+__device__ __forceinline__ void vel_pairs4(const float2* md, const float* y0, int ystep, float2& s0,
                                            float2& s1, float2& s2, float2& s3) {
   float2 c[4][NP];
 #pragma unroll
   for (int h = 0; h < NP; ++h) {
 #pragma unroll
-    for (int r = 0; r < 4; ++r) c[r][h] = __ldg(reinterpret_cast<const float2*>(y0 + r * ystep + 2 * h));
+    for (int r = 0; r < 4; ++r) c[r][h] = *reinterpret_cast<const float2*>(y0 + r * ystep + 2 * h);
   }
 #pragma unroll
   for (int h = 0; h < NP; ++h) {
@@ -219,6 +251,7 @@ __global__ void __launch_bounds__(1024) k_build_tiles(BuildArgs A) {
   __shared__ uint32_t obsmap[32][kNbWords];
   __shared__ float tab[32][8];
   uint16_t* const wcol = win + counter_col(warp, lane);
+  float* const ysm = reinterpret_cast<float*>(win + ((size_t)(kWinBins + 1) << log2S));  // rc x coeff_stride(nm)
 
   // the next layer's launch may start its CTAs once every CTA of this one has
   // started (programmatic dependent launch); it reads this layer's values only
@@ -267,31 +300,63 @@ __global__ void __launch_bounds__(1024) k_build_tiles(BuildArgs A) {
   // cells of S1 tests every S2 whose box with S1 contains it (rows beyond o
   // from S1, or all rows when o is on S1's row; the same for columns), so no
   // box is scanned once per S2; the tests and the bits are the same.
+  // The (cell, obstacle) pairs are first collected into a list (in the
+  // velocity buffer, unused until the realisation loop), then a warp takes a
+  // pair and spreads its tests over the lanes: a thread per pair left every
+  // warp waiting on its slowest lane (200x200x120 builder 361 -> 343 ms).
   {
     const int32_t* mT = A.F.mask + (int64_t)T * nc;
-    for (int idx = tid; idx < 32 * kNbBits; idx += nthr) {
-      const int c = idx / kNbBits, ob = idx - c * kNbBits;
-      const int64_t cc = c0 + c;
-      if (cc >= nc) continue;
-      const int da = ob / kNbSide - kNb, db = ob % kNbSide - kNb;
-      if (da == 0 && db == 0) continue;
-      const int ci1 = (int)(cc / g), cj1 = (int)(cc - (int64_t)ci1 * g);
-      const int oi = ci1 + da, oj = cj1 + db;
-      if (oi < 0 || oi >= g || oj < 0 || oj >= g) continue;
-      const int64_t sp = (int64_t)oj + (int64_t)g * oi;
-      if (!(__ldg(mT + sp) == 1 || __ldg(mT + nc + sp) == 1)) continue;
-      const int dilo = da > 0 ? da : -kNb, dihi = da < 0 ? da : kNb;
-      const int djlo = db > 0 ? db : -kNb, djhi = db < 0 ? db : kNb;
-      for (int di = dilo; di <= dihi; ++di) {
-        const int i2 = ci1 + di;
-        if (i2 < 0 || i2 >= g) continue;
-        for (int dj = djlo; dj <= djhi; ++dj) {
-          const int j2 = cj1 + dj;
-          if (j2 < 0 || j2 >= g) continue;
+    uint16_t* const pairs = reinterpret_cast<uint16_t*>(velw);  // entries c * kNbBits + ob
+    const int cap = min(32 * kNbBits, (int)((size_t)32 * vstride * sizeof(float2) / sizeof(uint16_t)));
+    __shared__ int npairs;
+    for (int s0 = 0; s0 < 32 * kNbBits; s0 += cap) {
+      const int s1 = min(s0 + cap, 32 * kNbBits);
+      if (tid == 0) npairs = 0;
+      __syncthreads();
+      for (int i0 = s0; i0 < s1; i0 += nthr) {  // the same trip count in every thread
+        const int idx = i0 + tid;
+        bool hit = false;
+        if (idx < s1) {
+          const int c = idx / kNbBits, ob = idx - c * kNbBits;
+          const int64_t cc = c0 + c;
+          const int da = ob / kNbSide - kNb, db = ob % kNbSide - kNb;
+          if (cc < nc && !(da == 0 && db == 0)) {
+            const int ci1 = (int)(cc / g), cj1 = (int)(cc - (int64_t)ci1 * g);
+            const int oi = ci1 + da, oj = cj1 + db;
+            if (oi >= 0 && oi < g && oj >= 0 && oj < g) {
+              const int64_t sp = (int64_t)oj + (int64_t)g * oi;
+              hit = __ldg(mT + sp) == 1 || __ldg(mT + nc + sp) == 1;
+            }
+          }
+        }
+        const unsigned bal = __ballot_sync(0xffffffffu, hit);
+        int at = 0;
+        if (lane == 0 && bal) at = atomicAdd(&npairs, __popc(bal));
+        at = __shfl_sync(0xffffffffu, at, 0);
+        if (hit) pairs[at + __popc(bal & ((1u << lane) - 1u))] = (uint16_t)idx;
+      }
+      __syncthreads();
+      const int n = npairs;
+      for (int pi = warp; pi < n; pi += nwarps) {
+        const int idx = pairs[pi];
+        const int c = idx / kNbBits, ob = idx - c * kNbBits;
+        const int64_t cc = c0 + c;
+        const int da = ob / kNbSide - kNb, db = ob % kNbSide - kNb;
+        const int ci1 = (int)(cc / g), cj1 = (int)(cc - (int64_t)ci1 * g);
+        const int oi = ci1 + da, oj = cj1 + db;
+        const int dilo = da > 0 ? da : -kNb, dihi = da < 0 ? da : kNb;
+        const int djlo = db > 0 ? db : -kNb, djhi = db < 0 ? db : kNb;
+        const int nj = djhi - djlo + 1, ntest = (dihi - dilo + 1) * nj;
+        for (int t = lane; t < ntest; t += 32) {
+          const int ti = t / nj;
+          const int di = dilo + ti, dj = djlo + (t - ti * nj);
+          const int i2 = ci1 + di, j2 = cj1 + dj;
+          if (i2 < 0 || i2 >= g || j2 < 0 || j2 >= g) continue;
           const int tb = (di + kNb) * kNbSide + (dj + kNb);
           if (within_band(P, oi, oj, ci1, cj1, i2, j2)) atomicOr(&obsmap[c][tb >> 5], 1u << (tb & 31));
         }
       }
+      __syncthreads();  // the list is consumed
     }
   }
 
@@ -320,7 +385,7 @@ __global__ void __launch_bounds__(1024) k_build_tiles(BuildArgs A) {
     mode = MODE_FIXED;  // obstacle S1: no move, r = r_outbound (:542-544)
     r_fixed = P.r_out;
   }
-  __syncthreads();  // obsmap complete
+  // obsmap is complete: the pair loop above ends with a barrier
   for (int b = 0; b <= kMissBin; ++b) wcol[b << log2S] = 0;
   int wi0 = 0, wj0 = 0;
   uint64_t ovr = 0, inwin = 0, edge = 0, term = 0, slow = 0;
@@ -404,7 +469,7 @@ __global__ void __launch_bounds__(1024) k_build_tiles(BuildArgs A) {
   const float2 FF = make_float2(F, F), csn = make_float2(cs, sn), dt2 = make_float2(dt, dt);
   const float2 xy1 = make_float2(x1, y1);
   const float2 sgn = make_float2(1.0f, -1.0f), org = make_float2(-xs0, ysn);
-  const bool y_pairs = (nm % 2 == 0) && ((reinterpret_cast<uintptr_t>(A.F.Y) & 7) == 0);
+  const bool y_pairs = (nm % 2 == 0);  // staged rows are 8-byte aligned
 
   // Rewards of the counted (in-window) samples of a row, from its counters.
   // Without a clamp a sample's reward depends only on its bin: r_outbound in an
@@ -510,24 +575,30 @@ __global__ void __launch_bounds__(1024) k_build_tiles(BuildArgs A) {
   };
 
   // ---- realisations in warp-private chunks ----------------------------------
+  // The chunk's coefficients (shared by all cells of the layer) are staged
+  // once per CTA: the next chunk's copies run while the warps count the
+  // current one (each warp loading them from L2: 200x200x120 builder 365 ms,
+  // staged: 361 ms).
+  const int ys = coeff_stride(nm);
+  const float* ylayer = A.F.Y + (int64_t)T * P.nrzns * nm;
+  stage_coeffs(ysm, ys, ylayer, min(rc, P.nrzns), nm, tid, nthr);
   for (int base = 0; base < P.nrzns; base += rc) {
     const int clen = min(rc, P.nrzns - base);
-    __syncwarp();  // previous chunk consumed
+    asm volatile("cp.async.wait_all;" ::: "memory");
+    __syncthreads();  // the chunk's coefficients are staged; the previous chunk is consumed
     // extract_velocity, src/build_model.cu:389-401: mean + sum over modes, both
     // sums as one chain of packed fused multiply-adds in the reference's order
     if (cvalid) {
       const float2* md = modes + cl;
-      const float* yb = A.F.Y + ((int64_t)T * P.nrzns + base) * nm;
-      const int64_t ystep = (int64_t)per * nm;
+      const float* yb = ysm;
+      const int ystep = per * ys;
       int q = a;
       // four of the lane's realisations at a time: each mode pair read from
       // shared memory feeds four independent chains.  For an even mode count
       // up to ten, vel_pairs4 issues every coefficient load of the four rows
-      // before the multiply-adds (one L2 round trip instead of one per mode
-      // pair: 200x200x120 builder 437 -> 414 ms, 300x300x150 545 -> 538 ms);
-      // the sums keep their order
+      // before the multiply-adds; the sums keep their order
       for (; q + 3 * per < clen; q += 4 * per) {
-        const float* y0 = yb + (int64_t)q * nm;
+        const float* y0 = yb + q * ys;
         float2 s0 = make_float2(0.f, 0.f), s1 = s0, s2 = s0, s3 = s0;
         if (y_pairs && nm <= 10) {  // nm even, rows 8-byte aligned: coefficients two at a time
           switch (nm >> 1) {
@@ -540,10 +611,10 @@ __global__ void __launch_bounds__(1024) k_build_tiles(BuildArgs A) {
         } else if (y_pairs) {
           for (int k = 0; k < nm; k += 2) {
             const float2 m0 = md[k * 32], m1 = md[(k + 1) * 32];
-            const float2 c0 = __ldg(reinterpret_cast<const float2*>(y0 + k));
-            const float2 c1 = __ldg(reinterpret_cast<const float2*>(y0 + ystep + k));
-            const float2 c2 = __ldg(reinterpret_cast<const float2*>(y0 + 2 * ystep + k));
-            const float2 c3 = __ldg(reinterpret_cast<const float2*>(y0 + 3 * ystep + k));
+            const float2 c0 = *reinterpret_cast<const float2*>(y0 + k);
+            const float2 c1 = *reinterpret_cast<const float2*>(y0 + ystep + k);
+            const float2 c2 = *reinterpret_cast<const float2*>(y0 + 2 * ystep + k);
+            const float2 c3 = *reinterpret_cast<const float2*>(y0 + 3 * ystep + k);
             s0 = __ffma2_rn(m0, make_float2(c0.x, c0.x), s0);
             s1 = __ffma2_rn(m0, make_float2(c1.x, c1.x), s1);
             s2 = __ffma2_rn(m0, make_float2(c2.x, c2.x), s2);
@@ -556,8 +627,8 @@ __global__ void __launch_bounds__(1024) k_build_tiles(BuildArgs A) {
         } else {
           for (int k = 0; k < nm; k++) {
             const float2 m0 = md[k * 32];
-            const float c0 = __ldg(y0 + k), c1 = __ldg(y0 + ystep + k);
-            const float c2 = __ldg(y0 + 2 * ystep + k), c3 = __ldg(y0 + 3 * ystep + k);
+            const float c0 = y0[k], c1 = y0[ystep + k];
+            const float c2 = y0[2 * ystep + k], c3 = y0[3 * ystep + k];
             s0 = __ffma2_rn(m0, make_float2(c0, c0), s0);
             s1 = __ffma2_rn(m0, make_float2(c1, c1), s1);
             s2 = __ffma2_rn(m0, make_float2(c2, c2), s2);
@@ -570,24 +641,26 @@ __global__ void __launch_bounds__(1024) k_build_tiles(BuildArgs A) {
         myvel[q + 3 * per] = make_float2(u1 + s3.x, v1 + s3.y);
       }
       for (; q < clen; q += per) {
-        const float* y = yb + (int64_t)q * nm;
+        const float* y = yb + q * ys;
         float2 sum = make_float2(0.f, 0.f);
         if (y_pairs) {
           for (int k = 0; k < nm; k += 2) {
-            const float2 yy = __ldg(reinterpret_cast<const float2*>(y + k));
+            const float2 yy = *reinterpret_cast<const float2*>(y + k);
             sum = __ffma2_rn(md[k * 32], make_float2(yy.x, yy.x), sum);
             sum = __ffma2_rn(md[(k + 1) * 32], make_float2(yy.y, yy.y), sum);
           }
         } else {
           for (int k = 0; k < nm; k++) {
-            const float yk = __ldg(y + k);
+            const float yk = y[k];
             sum = __ffma2_rn(md[k * 32], make_float2(yk, yk), sum);
           }
         }
         myvel[q] = make_float2(u1 + sum.x, v1 + sum.y);
       }
     }
-    __syncwarp();
+    __syncthreads();  // every warp has read the chunk's coefficients
+    if (base + rc < P.nrzns)
+      stage_coeffs(ysm, ys, ylayer + (int64_t)(base + rc) * nm, min(rc, P.nrzns - base - rc), nm, tid, nthr);
     if (mode == MODE_FIXED) {
       for (int q = 0; q < clen; ++q) sumR += r_fixed;
     } else if (mode == MODE_WINDOW) {
@@ -924,7 +997,8 @@ size_t build_smem_bytes(int na, int nm, int rc, bool unit) {
   const int nthr = 32 << build_lanes_log2(na);
   return (size_t)2 * nm * 32 * sizeof(float) + (size_t)32 * (rc + 2) * sizeof(float2) +
          (unit ? 0 : (size_t)MASK_COUNT * nthr * sizeof(uint64_t)) +
-         (size_t)(kWinBins + 1) * ((size_t)1 << counter_log2_stride(nthr)) * sizeof(uint16_t);
+         (size_t)(kWinBins + 1) * ((size_t)1 << counter_log2_stride(nthr)) * sizeof(uint16_t) +
+         (size_t)rc * coeff_stride(nm) * sizeof(float);
 }
 
 template <typename CntT, bool UNIT, bool FUSED = false>
