@@ -9,35 +9,35 @@
 //                       without contraction (:130-147, 20-84 for the cloud)
 //   k_env_center        column means in sample order (np.mean over axis 1 is a
 //                       sequential sum for this layout) and the centred matrix
-//   SVD                 of the centred matrix, the leading n_modes triplets:
-//                       a randomized range finder (n_modes + 10 columns, two
-//                       power iterations, QR by cuSOLVER, products by cuBLAS)
-//                       and a one-sided Jacobi SVD (cuSOLVER gesvdj) of the
-//                       projected matrix, accepted when the explicit residual
+//   rank reduction      the leading n_modes singular triplets of the centred
+//                       matrix by a randomized range finder (n_modes + 10
+//                       columns from a fixed hash, two power iterations) in
+//                       hand-written double kernels: products X B and X^T B,
+//                       Gram-Schmidt twice for the orthonormal bases, and the
+//                       SVD of the projected matrix through its QR factor and a
+//                       one-sided Jacobi SVD of that factor (relative accuracy,
+//                       like LAPACK's).  Accepted when the explicit residual
 //                       |X - Q Q^T X|_F is below 1e-10 s_1 (then every kept
-//                       singular value is exact to ~|R|^2/s_k); otherwise, as
-//                       at t = 0 where X is rounding noise, gesvdj of the whole
-//                       matrix.  Either way singular values come to about
-//                       machine precision relative to the largest, like
-//                       np.linalg.svd's LAPACK (a Gram-matrix eigensolve would
-//                       lose (s_1/s_k)^2 of it, and s_4/s_1 ~ 1e-6 here); the
-//                       first n_modes give coefficients u_k s_k and modes v_k,
-//                       signs fixed so that each coefficient column's
-//                       largest-magnitude entry is positive (the reference's
-//                       np.linalg.svd leaves the sign to LAPACK)
+//                       singular value is exact to ~|R|^2/s_k), or when s_1 is
+//                       below 1e-10 of the data's own size (the t = 0 matrices,
+//                       rounding noise of the centring, whose vectors no
+//                       implementation determines); otherwise re-run with twice
+//                       the columns and four power iterations.  The first
+//                       n_modes give coefficients u_k s_k and modes v_k, signs
+//                       fixed so that each coefficient column's largest-magnitude
+//                       entry is positive (the reference's np.linalg.svd leaves
+//                       the sign to LAPACK)
 // then, for all steps, k_env_interpolate: the reference's griddata 'linear' on
 // the coarse cell centres, evaluated from a table of (triangle vertices,
 // barycentric weights) per fine point that the caller builds from the same
 // Delaunay triangulation (scipy's), summed in griddata's order in double
 // without contraction; points outside the hull read 0 (np.nan_to_num of the
 // fill value).
-#include <cublas_v2.h>
 #include <cuda_runtime.h>
-#include <cusolverDn.h>
 #include <math.h>
 
 #include <algorithm>
-#include <mutex>
+#include <cmath>
 #include <string>
 #include <vector>
 
@@ -51,19 +51,6 @@ using namespace e2e;
     cudaError_t _e = (call);                            \
     if (_e != cudaSuccess) return cuda_fail(_e, #call); \
   } while (0)
-#define CKB(call)                                                                               \
-  do {                                                                                          \
-    cublasStatus_t _s = (call);                                                                 \
-    if (_s != CUBLAS_STATUS_SUCCESS)                                                            \
-      return fail(E2E_ERR_CUDA, std::string(#call) + ": cuBLAS status " + std::to_string((int)_s)); \
-  } while (0)
-#define CKS(call)                                                                           \
-  do {                                                                                      \
-    cusolverStatus_t _s = (call);                                                           \
-    if (_s != CUSOLVER_STATUS_SUCCESS)                                                      \
-      return fail(E2E_ERR_CUDA, std::string(#call) + ": cuSOLVER status " + std::to_string((int)_s)); \
-  } while (0)
-
 namespace {
 
 constexpr double kPi = 3.141592653589793;  // math.pi
@@ -193,14 +180,6 @@ __global__ void k_env_test_matrix(double* O, int64_t n) {
   O[i] = (double)(z >> 11) * (2.0 / 9007199254740992.0) - 1.0;
 }
 
-// row-major nws x ncols -> column-major (ld nws)
-__global__ void k_env_transpose(const double* X, int nws, int ncols, double* B) {
-  const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (idx >= (int64_t)nws * ncols) return;
-  const int k = (int)(idx / ncols), c = (int)(idx - (int64_t)k * ncols);
-  B[(int64_t)c * nws + k] = X[idx];
-}
-
 // coarse arrays of step t: [u, v, phi, ui_0.., vi_0.., phi_i_0..] (3 + 3r arrays
 // of n) and the coefficients of both rank reductions.  The reference holds the
 // coarse means and modes in float32 arrays except all_phi_mat, a float64 array
@@ -322,131 +301,465 @@ __global__ void k_env_cloud(CloudArgs a) {
   a.mask[idx] = m;
 }
 
-// Truncated SVD of the centred nws x ncols matrix X (row-major, on the device;
-// destroyed) by one-sided Jacobi (cuSOLVER gesvdj, economy size, sorted): the
-// row-major buffer is the column-major ncols x nws matrix X^T, which gesvdj
-// takes directly when ncols >= nws (X^T = U S V^T: X's left vectors are V);
-// otherwise X is transposed into column-major nws x ncols first.
-// cuSOLVER and cuBLAS handles, one pair per device for the whole process,
-// created on first use and kept until exit (never destroyed: a destructor at
-// process exit could run after the CUDA context is gone).  A call holds the
-// device's mutex while it uses them, so calls from any number of host
-// threads share one pair and one work space; generations on one device run
-// one at a time.  Creating the handles on every call allocated their device
-// work space through the driver each time, which on a busy machine added tens
-// of milliseconds to a 35 ms generation.  The handles belong to the device's
-// primary context: after cudaDeviceReset the process must not generate again.
-struct DevHandles {
-  std::mutex mu;
-  cusolverDnHandle_t sol = nullptr;
-  cublasHandle_t blas = nullptr;
-};
-DevHandles g_handles[64];
+// ---- rank reduction: the leading singular triplets of the centred matrix ----
+//
+// X is row-major nws x ncols on the device.  A randomized range finder with k
+// columns (n_modes + 10): Q = orth(X Om), two power iterations
+// Q <- orth(X orth(X^T Q)), Bt = X^T Q (ncols x k), the explicit residual
+// |X - Q Bt^T|_F, then the SVD of Bt through its QR: Bt = Qb R, R = U_R S V_R^T
+// by one-sided Jacobi (relative accuracy: each singular value of R equals one
+// of Bt's to about eps s_1, so a Gram-matrix eigensolve's (s_1/s_k)^2 loss is
+// avoided), Ub = Qb U_R, and the sample-side vectors L = Q V_R.  Every product
+// and reduction runs in a fixed order (warp trees, segment sums in segment
+// order), so a generation is deterministic.  Matrices besides X are
+// column-major with the leading dimension of their row count.
 
-e2e_status solver_handles(cusolverDnHandle_t* sol, cublasHandle_t* blas, std::unique_lock<std::mutex>* hold) {
-  int dev = 0;
-  cudaError_t e = cudaGetDevice(&dev);
-  if (e != cudaSuccess) return cuda_fail(e, "cudaGetDevice");
-  if (dev < 0 || dev >= 64) return fail(E2E_ERR_UNSUPPORTED, "device index above 63");
-  DevHandles& x = g_handles[dev];
-  std::unique_lock<std::mutex> lk(x.mu);
-  if (!x.sol && cusolverDnCreate(&x.sol) != CUSOLVER_STATUS_SUCCESS) {
-    x.sol = nullptr;
-    return fail(E2E_ERR_CUDA, "cusolverDnCreate");
+constexpr int kRrMaxK = 64;       // range-finder columns at most
+constexpr int kRrMaxSweeps = 60;  // Jacobi sweeps at most (convergence is quadratic)
+
+// partial products of X^T B over row segments: P[seg][c][j] = sum over the
+// segment's rows i, in order, of X[i][j] B[i][c]; a thread per column j
+template <int K>
+__global__ void __launch_bounds__(128) k_rr_xtb(const double* X, int nws, int ncols, const double* B, int ldb,
+                                                int k, int seg_rows, double* P) {
+  __shared__ double Bs[32][K];
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  const int i0 = blockIdx.y * seg_rows, i1 = min(nws, i0 + seg_rows);
+  double acc[K];
+#pragma unroll
+  for (int c = 0; c < K; ++c) acc[c] = 0.0;
+  for (int it = i0; it < i1; it += 32) {
+    const int nrow = min(32, i1 - it);
+    __syncthreads();
+    for (int e = threadIdx.x; e < 32 * K; e += blockDim.x) {
+      const int rr = e / K, c = e - rr * K;
+      Bs[rr][c] = (rr < nrow && c < k) ? B[(int64_t)c * ldb + it + rr] : 0.0;
+    }
+    __syncthreads();
+    if (j < ncols) {
+      for (int rr = 0; rr < nrow; ++rr) {
+        const double x = X[(int64_t)(it + rr) * ncols + j];
+#pragma unroll
+        for (int c = 0; c < K; ++c) acc[c] = fma(x, Bs[rr][c], acc[c]);
+      }
+    }
   }
-  if (!x.blas && cublasCreate(&x.blas) != CUBLAS_STATUS_SUCCESS) {
-    x.blas = nullptr;
-    return fail(E2E_ERR_CUDA, "cublasCreate");
+  if (j < ncols) {
+#pragma unroll
+    for (int c = 0; c < K; ++c)
+      if (c < k) P[((int64_t)blockIdx.y * k + c) * ncols + j] = acc[c];
   }
-  *sol = x.sol;
-  *blas = x.blas;
-  *hold = std::move(lk);
-  return E2E_OK;
+}
+
+// C[j + c ldc] = sum over segments s = 0.. in order of P[s][c][j]
+__global__ void k_rr_sum_segments(const double* P, int nseg, int ncols, int k, double* C, int ldc) {
+  const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= (int64_t)ncols * k) return;
+  const int c = (int)(e / ncols), j = (int)(e - (int64_t)c * ncols);
+  double s = P[(int64_t)c * ncols + j];
+  for (int g = 1; g < nseg; ++g) s += P[((int64_t)g * k + c) * ncols + j];
+  C[(int64_t)c * ldc + j] = s;
+}
+
+// C (nws x k) = X B, B ncols x k: a warp per row of X, lanes over its columns,
+// lane sums reduced by a shuffle tree (lane 0's result is written)
+template <int K>
+__global__ void __launch_bounds__(256) k_rr_xb(const double* X, int nws, int ncols, const double* B, int ldb,
+                                               int k, double* C, int ldc) {
+  const int row = (int)(((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5), lane = threadIdx.x & 31;
+  if (row >= nws) return;  // whole warps
+  double acc[K];
+#pragma unroll
+  for (int c = 0; c < K; ++c) acc[c] = 0.0;
+  const double* x = X + (int64_t)row * ncols;
+  for (int j = lane; j < ncols; j += 32) {
+    const double xv = x[j];
+#pragma unroll
+    for (int c = 0; c < K; ++c)
+      if (c < k) acc[c] = fma(xv, B[(int64_t)c * ldb + j], acc[c]);
+  }
+#pragma unroll
+  for (int c = 0; c < K; ++c) {
+    if (c < k) {
+      double v = acc[c];
+      for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+      if (lane == 0) C[(int64_t)c * ldc + row] = v;
+    }
+  }
+}
+
+// C (rows x k) = A (rows x k) W (k x k, ld k): a thread per entry, sum in order
+__global__ void k_rr_small(const double* A, int lda, int rows, int k, const double* W, double* C, int ldc) {
+  const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= (int64_t)rows * k) return;
+  const int c = (int)(e / rows), i = (int)(e - (int64_t)c * rows);
+  double s = 0.0;
+  for (int l = 0; l < k; ++l) s = fma(A[(int64_t)l * lda + i], W[l + c * k], s);
+  C[(int64_t)c * ldc + i] = s;
+}
+
+// block-wide sum of v (fixed order: a shuffle tree per warp, then the warps in
+// order by thread 0); every thread returns it.  red: 33 doubles of shared memory
+__device__ double rr_block_sum(double v, double* red) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  __syncthreads();
+  if (lane == 0) red[warp] = v;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double s = red[0];
+    for (int w = 1; w < nw; ++w) s += red[w];
+    red[32] = s;
+  }
+  __syncthreads();
+  return red[32];
+}
+
+// Orthonormal columns in place: A (rows x k, ld lda) = Q R by classical
+// Gram-Schmidt applied twice per column (orthogonal to working precision); R
+// (k x k, ld k, upper triangular, may be null) receives both passes'
+// coefficients and the norms.  A column that the second pass shrinks below
+// half its length lies in the span of the earlier ones to working precision
+// (what is left is rounding, which no further pass makes orthogonal): it
+// becomes zero, as does a zero column (R's diagonal 0).  One CTA.
+template <int K>
+__global__ void __launch_bounds__(256) k_rr_cgs2(double* A, int rows, int k, int lda, double* R) {
+  __shared__ double red[33];
+  __shared__ double wsum[8][K];
+  __shared__ double d[K];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nw = blockDim.x >> 5;
+  if (R)
+    for (int e = tid; e < k * k; e += blockDim.x) R[e] = 0.0;
+  __syncthreads();
+  for (int j = 0; j < k; ++j) {
+    double* aj = A + (int64_t)j * lda;
+    double n1 = 0.0;  // length after the first pass
+    for (int pass = 0; pass < 2 && j > 0; ++pass) {
+      double part[K];
+#pragma unroll
+      for (int i = 0; i < K; ++i) part[i] = 0.0;
+      for (int row = tid; row < rows; row += blockDim.x) {
+        const double v = aj[row];
+#pragma unroll
+        for (int i = 0; i < K; ++i)
+          if (i < j) part[i] = fma(A[(int64_t)i * lda + row], v, part[i]);
+      }
+#pragma unroll
+      for (int i = 0; i < K; ++i) {
+        if (i < j) {
+          double v = part[i];
+          for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+          if (lane == 0) wsum[warp][i] = v;
+        }
+      }
+      __syncthreads();
+      if (tid < j) {
+        double s = wsum[0][tid];
+        for (int w = 1; w < nw; ++w) s += wsum[w][tid];
+        d[tid] = s;
+        if (R) R[tid + j * k] += s;
+      }
+      __syncthreads();
+      for (int row = tid; row < rows; row += blockDim.x) {
+        double v = aj[row];
+        for (int i = 0; i < j; ++i) v = fma(-d[i], A[(int64_t)i * lda + row], v);
+        aj[row] = v;
+      }
+      __syncthreads();
+      if (pass == 0) {
+        double t2 = 0.0;
+        for (int row = tid; row < rows; row += blockDim.x) t2 = fma(aj[row], aj[row], t2);
+        n1 = sqrt(rr_block_sum(t2, red));
+      }
+    }
+    double s2 = 0.0;
+    for (int row = tid; row < rows; row += blockDim.x) s2 = fma(aj[row], aj[row], s2);
+    const double n2 = sqrt(rr_block_sum(s2, red));
+    const double nrm = (j > 0 && n2 < 0.5 * n1) ? 0.0 : n2;
+    if (R && tid == 0) R[j + j * k] = nrm;
+    for (int row = tid; row < rows; row += blockDim.x) aj[row] = nrm > 0.0 ? aj[row] / nrm : 0.0;
+    __syncthreads();
+  }
+}
+
+// One-sided Jacobi SVD of the k x k matrix W (ld k, destroyed): its columns are
+// rotated until pairwise orthogonal (|w_p . w_q| <= k eps |w_p| |w_q|), the
+// rotations accumulated in V; then W_in = U diag(S) V^T.  Outputs sorted by
+// descending singular value (ties: lower column first): S (k), U and Vs (k x k,
+// ld k; a zero singular value gives a zero U column).  Rounds of disjoint
+// pairs (a round-robin tournament over the columns), a warp per pair, each
+// warp's reductions broadcast from lane 0 so all lanes rotate alike.  One CTA.
+__global__ void __launch_bounds__(256) k_rr_jacobi(double* W, double* V, int k, double* S, double* U, double* Vs,
+                                                   int* sweeps) {
+  __shared__ int rotated;
+  __shared__ double sv[kRrMaxK];
+  __shared__ int order[kRrMaxK];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nw = blockDim.x >> 5;
+  for (int e = tid; e < k * k; e += blockDim.x) V[e] = (e % k == e / k) ? 1.0 : 0.0;
+  const int kk = k + (k & 1);  // players (index k: a bye)
+  const double tol = (double)k * 2.220446049250313e-16;
+  int sweep = 0;
+  for (; sweep < kRrMaxSweeps; ++sweep) {
+    if (tid == 0) rotated = 0;
+    __syncthreads();
+    for (int round = 0; round < kk - 1; ++round) {
+      for (int pi = warp; pi < kk / 2; pi += nw) {
+        // position 0 holds player 0, position i >= 1 player 1 + (i - 1 + round) mod (kk - 1)
+        const int ia = pi, ib = kk - 1 - pi;
+        const int pa = ia == 0 ? 0 : 1 + (ia - 1 + round) % (kk - 1);
+        const int pb = 1 + (ib - 1 + round) % (kk - 1);
+        if (pa >= k || pb >= k) continue;
+        const int p = min(pa, pb), q = max(pa, pb);
+        double* wp = W + p * k;
+        double* wq = W + q * k;
+        double al = 0.0, be = 0.0, ga = 0.0;
+        for (int r = lane; r < k; r += 32) {
+          al = fma(wp[r], wp[r], al);
+          be = fma(wq[r], wq[r], be);
+          ga = fma(wp[r], wq[r], ga);
+        }
+        for (int o = 16; o > 0; o >>= 1) {
+          al += __shfl_xor_sync(0xffffffffu, al, o);
+          be += __shfl_xor_sync(0xffffffffu, be, o);
+          ga += __shfl_xor_sync(0xffffffffu, ga, o);
+        }
+        al = __shfl_sync(0xffffffffu, al, 0);
+        be = __shfl_sync(0xffffffffu, be, 0);
+        ga = __shfl_sync(0xffffffffu, ga, 0);
+        if (!(fabs(ga) > tol * sqrt(al) * sqrt(be))) continue;
+        const double zeta = (be - al) / (2.0 * ga);
+        const double t = fabs(zeta) > 1e150 ? 0.5 / zeta
+                                            : copysign(1.0, zeta) / (fabs(zeta) + sqrt(fma(zeta, zeta, 1.0)));
+        const double c = 1.0 / sqrt(fma(t, t, 1.0)), s = c * t;
+        double* vp = V + p * k;
+        double* vq = V + q * k;
+        for (int r = lane; r < k; r += 32) {
+          const double a = wp[r], b = wq[r];
+          wp[r] = c * a - s * b;
+          wq[r] = s * a + c * b;
+          const double va = vp[r], vb = vq[r];
+          vp[r] = c * va - s * vb;
+          vq[r] = s * va + c * vb;
+        }
+        if (lane == 0) rotated = 1;
+      }
+      __syncthreads();
+    }
+    const int any = rotated;
+    __syncthreads();
+    if (!any) break;
+  }
+  for (int j = tid; j < k; j += blockDim.x) {
+    double s2 = 0.0;
+    for (int r = 0; r < k; ++r) s2 = fma(W[j * k + r], W[j * k + r], s2);
+    sv[j] = sqrt(s2);
+  }
+  __syncthreads();
+  if (tid == 0) {
+    for (int j = 0; j < k; ++j) order[j] = j;
+    for (int a = 0; a < k; ++a) {
+      int best = a;
+      for (int b = a + 1; b < k; ++b)
+        if (sv[order[b]] > sv[order[best]] || (sv[order[b]] == sv[order[best]] && order[b] < order[best])) best = b;
+      const int tmp = order[a];
+      order[a] = order[best];
+      order[best] = tmp;
+    }
+    if (sweeps) *sweeps = sweep;
+  }
+  __syncthreads();
+  for (int e = tid; e < k * k; e += blockDim.x) {
+    const int c = e / k, r = e - c * k, src = order[c];
+    const double s = sv[src];
+    if (r == 0) S[c] = s;
+    U[e] = s > 0.0 ? W[src * k + r] / s : 0.0;
+    Vs[e] = V[src * k + r];
+  }
+}
+
+// partial sums of squares of the residual X - Q Bt^T (Q nws x k, Bt ncols x
+// k): a thread per column j over a row segment, one partial per CTA
+template <int K>
+__global__ void __launch_bounds__(128) k_rr_resid(const double* X, int nws, int ncols, const double* Q,
+                                                  const double* Bt, int k, int seg_rows, double* part) {
+  __shared__ double Qs[32][K];
+  __shared__ double red[33];
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  const int i0 = blockIdx.y * seg_rows, i1 = min(nws, i0 + seg_rows);
+  double b[K];
+#pragma unroll
+  for (int c = 0; c < K; ++c) b[c] = (j < ncols && c < k) ? Bt[(int64_t)c * ncols + j] : 0.0;
+  double ssq = 0.0;
+  for (int it = i0; it < i1; it += 32) {
+    const int nrow = min(32, i1 - it);
+    __syncthreads();
+    for (int e = threadIdx.x; e < 32 * K; e += blockDim.x) {
+      const int rr = e / K, c = e - rr * K;
+      Qs[rr][c] = (rr < nrow && c < k) ? Q[(int64_t)c * nws + it + rr] : 0.0;
+    }
+    __syncthreads();
+    if (j < ncols) {
+      for (int rr = 0; rr < nrow; ++rr) {
+        double v = X[(int64_t)(it + rr) * ncols + j];
+#pragma unroll
+        for (int c = 0; c < K; ++c) v = fma(-Qs[rr][c], b[c], v);
+        ssq = fma(v, v, ssq);
+      }
+    }
+  }
+  const double s = rr_block_sum(ssq, red);
+  if (threadIdx.x == 0) part[(int64_t)blockIdx.y * gridDim.x + blockIdx.x] = s;
+}
+
+// out[slot] = sum of v[0..n) in order (one thread: a few hundred partials)
+__global__ void k_rr_sum_serial(const double* v, int n, double* out, int slot) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  double s = 0.0;
+  for (int i = 0; i < n; ++i) s += v[i];
+  out[slot] = s;
+}
+
+// out[slot] = sum of squares of v[0..n), one CTA, fixed order
+__global__ void __launch_bounds__(256) k_rr_sumsq(const double* v, int n, double* out, int slot) {
+  __shared__ double red[33];
+  double s = 0.0;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) s = fma(v[i], v[i], s);
+  s = rr_block_sum(s, red);
+  if (threadIdx.x == 0) out[slot] = s;
 }
 
 struct SvdWork {
-  cusolverDnHandle_t sol = nullptr;
-  cublasHandle_t blas = nullptr;
-  gesvdjInfo_t params = nullptr;
-  // randomized range finder: k = r + oversampling columns
-  int k = 0;
-  double *Om = nullptr, *Q = nullptr, *Z = nullptr, *Bt = nullptr, *L = nullptr, *R = nullptr;
-  double *Ub = nullptr, *Vb = nullptr, *Sb = nullptr, *tau = nullptr;
-  double* qwork = nullptr;
-  int lqwork = 0;
-  double* B = nullptr;  // transposed copy (nws > ncols)
-  double* U = nullptr;  // m x min(m, n)
-  double* V = nullptr;  // n x min(m, n)
-  double* S = nullptr;  // min(m, n)
-  double* work = nullptr;
-  int lwork = 0;
-  int* info = nullptr;
+  int kmax = 0;      // columns the buffers hold
+  int ncols_max = 0;
+  double *Om = nullptr, *Q = nullptr, *Z = nullptr, *Bt = nullptr, *L = nullptr, *Ub = nullptr;
+  double *R = nullptr, *V = nullptr, *U = nullptr, *Vs = nullptr, *S = nullptr;
+  double* P = nullptr;     // segment partials: kRrSegs x ncols_max x kmax
+  double* part = nullptr;  // residual partials
+  int part_cap = 0;
+  double* scal = nullptr;  // device: [0] residual^2, [1] |mean|^2
+  double hscal[3] = {0.0, 0.0, 0.0};  // host copy of scal and S[0]
+  int* sweeps = nullptr;
 };
 
-e2e_status svd_shape(int nws, int ncols, int* m, int* n) {
-  if (ncols >= nws) {
-    *m = ncols;
-    *n = nws;
-  } else {
-    *m = nws;
-    *n = ncols;
+constexpr int kRrSegs = 16;  // row segments of the X^T B products at most
+
+int rr_bucket(int k) { return k <= 16 ? 16 : (k <= 32 ? 32 : 64); }
+
+// row segments for X^T B / the residual: enough CTAs to cover the SMs
+void rr_segments(int nws, int ncols, int* nseg, int* seg_rows) {
+  const int colblocks = (ncols + 127) / 128;
+  int s = std::max(1, std::min(kRrSegs, (296 + colblocks - 1) / colblocks));
+  s = std::min(s, (nws + 31) / 32);
+  int rows = (nws + s - 1) / s;
+  rows = (rows + 31) / 32 * 32;
+  *seg_rows = rows;
+  *nseg = (nws + rows - 1) / rows;
+}
+
+// C (ncols x k, ld ncols) = X^T B (B nws x k, ld nws)
+e2e_status rr_xtb(SvdWork& w, const double* X, int nws, int ncols, const double* B, int k, double* C,
+                  cudaStream_t st) {
+  int nseg, seg_rows;
+  rr_segments(nws, ncols, &nseg, &seg_rows);
+  const dim3 grid((unsigned)((ncols + 127) / 128), (unsigned)nseg);
+  switch (rr_bucket(k)) {
+    case 16: k_rr_xtb<16><<<grid, 128, 0, st>>>(X, nws, ncols, B, nws, k, seg_rows, w.P); break;
+    case 32: k_rr_xtb<32><<<grid, 128, 0, st>>>(X, nws, ncols, B, nws, k, seg_rows, w.P); break;
+    default: k_rr_xtb<64><<<grid, 128, 0, st>>>(X, nws, ncols, B, nws, k, seg_rows, w.P); break;
   }
+  CK(cudaGetLastError());
+  const int64_t ne = (int64_t)ncols * k;
+  k_rr_sum_segments<<<(unsigned)((ne + 255) / 256), 256, 0, st>>>(w.P, nseg, ncols, k, C, ncols);
+  CK(cudaGetLastError());
   return E2E_OK;
 }
 
-// orthonormal basis of the column range of A (rows x k, column-major, ld rows), in place
-e2e_status orthonormalize(SvdWork& w, double* A, int rows, int k) {
-  CKS(cusolverDnDgeqrf(w.sol, rows, k, A, rows, w.tau, w.qwork, w.lqwork, w.info));
-  CKS(cusolverDnDorgqr(w.sol, rows, k, k, A, rows, w.tau, w.qwork, w.lqwork, w.info));
+// C (nws x k, ld nws) = X B (B ncols x k, ld ncols)
+e2e_status rr_xb(const double* X, int nws, int ncols, const double* B, int k, double* C, cudaStream_t st) {
+  const unsigned blocks = (unsigned)(((int64_t)nws * 32 + 255) / 256);
+  switch (rr_bucket(k)) {
+    case 16: k_rr_xb<16><<<blocks, 256, 0, st>>>(X, nws, ncols, B, ncols, k, C, nws); break;
+    case 32: k_rr_xb<32><<<blocks, 256, 0, st>>>(X, nws, ncols, B, ncols, k, C, nws); break;
+    default: k_rr_xb<64><<<blocks, 256, 0, st>>>(X, nws, ncols, B, ncols, k, C, nws); break;
+  }
+  CK(cudaGetLastError());
   return E2E_OK;
 }
 
-// Randomized SVD of X (row-major nws x ncols, read only).  Returns false in
-// *ok when the residual check fails (the caller then runs gesvdj).
-e2e_status randomized_svd(SvdWork& w, const double* X, int nws, int ncols, int r, double* C, double* M,
-                          double* svals, bool* ok, cudaStream_t st) {
+e2e_status rr_orth(double* A, int rows, int k, double* R, cudaStream_t st) {
+  switch (rr_bucket(k)) {
+    case 16: k_rr_cgs2<16><<<1, 256, 0, st>>>(A, rows, k, rows, R); break;
+    case 32: k_rr_cgs2<32><<<1, 256, 0, st>>>(A, rows, k, rows, R); break;
+    default: k_rr_cgs2<64><<<1, 256, 0, st>>>(A, rows, k, rows, R); break;
+  }
+  CK(cudaGetLastError());
+  return E2E_OK;
+}
+
+// |X - Q Bt^T|_F^2 into w.scal[0]
+e2e_status rr_residual(SvdWork& w, const double* X, int nws, int ncols, int k, cudaStream_t st) {
+  int nseg, seg_rows;
+  rr_segments(nws, ncols, &nseg, &seg_rows);
+  const dim3 grid((unsigned)((ncols + 127) / 128), (unsigned)nseg);
+  const int np = (int)(grid.x * grid.y);
+  if (np > w.part_cap) return fail(E2E_ERR_INVALID, "residual partials above capacity");
+  switch (rr_bucket(k)) {
+    case 16: k_rr_resid<16><<<grid, 128, 0, st>>>(X, nws, ncols, w.Q, w.Bt, k, seg_rows, w.part); break;
+    case 32: k_rr_resid<32><<<grid, 128, 0, st>>>(X, nws, ncols, w.Q, w.Bt, k, seg_rows, w.part); break;
+    default: k_rr_resid<64><<<grid, 128, 0, st>>>(X, nws, ncols, w.Q, w.Bt, k, seg_rows, w.part); break;
+  }
+  CK(cudaGetLastError());
+  k_rr_sum_serial<<<1, 32, 0, st>>>(w.part, np, w.scal, 0);
+  CK(cudaGetLastError());
+  return E2E_OK;
+}
+
+// Randomized SVD of the centred X (row-major nws x ncols) with k columns and
+// `power` power iterations; *ok when certified:
+//  * |X - Q Q^T X|_F <= 1e-10 s_1 (then each kept singular value is exact to
+//    about |R|^2 / s_k, machine precision relative to s_1), or
+//  * s_1 <= 1e-10 sqrt(nws) |mean|: the centred matrix is below the rounding of
+//    the data it was centred from (every realisation alike, as at t = 0), so
+//    its singular vectors are not determined by the data and the computed ones
+//    stand, as LAPACK's do for the reference.
+e2e_status randomized_svd(SvdWork& w, const double* X, int nws, int ncols, int r, int k, int power,
+                          const double* mean, double* C, double* M, double* svals, bool* ok, cudaStream_t st) {
   *ok = false;
-  const int k = std::min(w.k, std::min(nws, ncols));
-  if (k <= r || (int64_t)nws * ncols > (int64_t)0x7fffffff) return E2E_OK;
-  const double one = 1.0, zero = 0.0, mone = -1.0;
-  // X as the column-major ncols x nws matrix Xc (= X^T), ld ncols
   const int64_t no = (int64_t)ncols * k;
   k_env_test_matrix<<<(unsigned)((no + 255) / 256), 256, 0, st>>>(w.Om, no);
   CK(cudaGetLastError());
-  // Q = X Om (nws x k)
-  CKB(cublasDgemm(w.blas, CUBLAS_OP_T, CUBLAS_OP_N, nws, k, ncols, &one, X, ncols, w.Om, ncols, &zero, w.Q, nws));
-  e2e_status s = orthonormalize(w, w.Q, nws, k);
-  if (s != E2E_OK) return s;
-  for (int it = 0; it < 2; ++it) {  // power iterations: Q <- orth(X orth(X^T Q))
-    CKB(cublasDgemm(w.blas, CUBLAS_OP_N, CUBLAS_OP_N, ncols, k, nws, &one, X, ncols, w.Q, nws, &zero, w.Z, ncols));
-    s = orthonormalize(w, w.Z, ncols, k);
-    if (s != E2E_OK) return s;
-    CKB(cublasDgemm(w.blas, CUBLAS_OP_T, CUBLAS_OP_N, nws, k, ncols, &one, X, ncols, w.Z, ncols, &zero, w.Q, nws));
-    s = orthonormalize(w, w.Q, nws, k);
-    if (s != E2E_OK) return s;
+  e2e_status s;
+  if ((s = rr_xb(X, nws, ncols, w.Om, k, w.Q, st)) != E2E_OK) return s;     // Q = X Om
+  if ((s = rr_orth(w.Q, nws, k, nullptr, st)) != E2E_OK) return s;
+  for (int it = 0; it < power; ++it) {                                        // Q <- orth(X orth(X^T Q))
+    if ((s = rr_xtb(w, X, nws, ncols, w.Q, k, w.Z, st)) != E2E_OK) return s;
+    if ((s = rr_orth(w.Z, ncols, k, nullptr, st)) != E2E_OK) return s;
+    if ((s = rr_xb(X, nws, ncols, w.Z, k, w.Q, st)) != E2E_OK) return s;
+    if ((s = rr_orth(w.Q, nws, k, nullptr, st)) != E2E_OK) return s;
   }
-  // Bt = X^T Q (ncols x k) = (Q^T X)^T
-  CKB(cublasDgemm(w.blas, CUBLAS_OP_N, CUBLAS_OP_N, ncols, k, nws, &one, X, ncols, w.Q, nws, &zero, w.Bt, ncols));
-  // residual X - Q Q^T X, as Xc - Bt Q^T, and its Frobenius norm
-  CK(cudaMemcpyAsync(w.R, X, sizeof(double) * (size_t)nws * ncols, cudaMemcpyDeviceToDevice, st));
-  CKB(cublasDgemm(w.blas, CUBLAS_OP_N, CUBLAS_OP_T, ncols, nws, k, &mone, w.Bt, ncols, w.Q, nws, &one, w.R, ncols));
-  double rnorm = 0.0;
-  CKB(cublasDnrm2(w.blas, nws * ncols, w.R, 1, &rnorm));  // host result: synchronises
-  // SVD of the tall Bt = Ub S Vb^T: X ~ Q B = (Q Vb) S Ub^T
-  CKS(cusolverDnDgesvdj(w.sol, CUSOLVER_EIG_MODE_VECTOR, 1, ncols, k, w.Bt, ncols, w.Sb, w.Ub, ncols, w.Vb, k,
-                        w.work, w.lwork, w.info, w.params));
-  int h_info = 0;
-  CK(cudaMemcpyAsync(&h_info, w.info, sizeof(int), cudaMemcpyDeviceToHost, st));
-  double s1 = 0.0;
-  CK(cudaMemcpyAsync(&s1, w.Sb, sizeof(double), cudaMemcpyDeviceToHost, st));
+  if ((s = rr_xtb(w, X, nws, ncols, w.Q, k, w.Bt, st)) != E2E_OK) return s;  // Bt = X^T Q
+  if ((s = rr_residual(w, X, nws, ncols, k, st)) != E2E_OK) return s;
+  k_rr_sumsq<<<1, 256, 0, st>>>(mean, ncols, w.scal, 1);
+  CK(cudaGetLastError());
+  // Bt = Qb R (Bt becomes Qb), R = U_R S V_R^T, Ub = Qb U_R, L = Q V_R
+  if ((s = rr_orth(w.Bt, ncols, k, w.R, st)) != E2E_OK) return s;
+  k_rr_jacobi<<<1, 256, 0, st>>>(w.R, w.V, k, w.S, w.U, w.Vs, w.sweeps);
+  CK(cudaGetLastError());
+  const int64_t nu = (int64_t)ncols * k, nl = (int64_t)nws * k;
+  k_rr_small<<<(unsigned)((nu + 255) / 256), 256, 0, st>>>(w.Bt, ncols, ncols, k, w.U, w.Ub, ncols);
+  k_rr_small<<<(unsigned)((nl + 255) / 256), 256, 0, st>>>(w.Q, nws, nws, k, w.Vs, w.L, nws);
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(w.hscal, w.scal, 2 * sizeof(double), cudaMemcpyDeviceToHost, st));
+  CK(cudaMemcpyAsync(w.hscal + 2, w.S, sizeof(double), cudaMemcpyDeviceToHost, st));
   CK(cudaStreamSynchronize(st));
-  if (h_info != 0 || !(rnorm <= 1e-10 * s1) || !(s1 > 0.0)) return E2E_OK;
-  CKB(cublasDgemm(w.blas, CUBLAS_OP_N, CUBLAS_OP_N, nws, k, k, &one, w.Q, nws, w.Vb, k, &zero, w.L, nws));
+  const double rnorm = sqrt(w.hscal[0]), mnorm = sqrt(w.hscal[1]), s1 = w.hscal[2];
+  const bool certified = (s1 > 0.0 && rnorm <= 1e-10 * s1) || !(s1 > 1e-10 * sqrt((double)nws) * mnorm);
+  if (!certified || !std::isfinite(rnorm) || !std::isfinite(s1)) return E2E_OK;
   ModeArgs a;
   a.nws = nws;
   a.ncols = ncols;
   a.r = r;
-  a.S = w.Sb;
+  a.S = w.S;
   a.Us = w.L;
   a.ldu = nws;
   a.Vs = w.Ub;
@@ -460,50 +773,29 @@ e2e_status randomized_svd(SvdWork& w, const double* X, int nws, int ncols, int r
   return E2E_OK;
 }
 
-e2e_status truncated_svd(SvdWork& w, double* X, int nws, int ncols, int r, double* C, double* M, double* svals,
-                         cudaStream_t st, int* full_svds) {
-  bool ok = false;
-  e2e_status rs = randomized_svd(w, X, nws, ncols, r, C, M, svals, &ok, st);
-  if (rs != E2E_OK) return rs;
-  if (ok) return E2E_OK;
-  ++*full_svds;
-  int m, n;
-  svd_shape(nws, ncols, &m, &n);
-  double* A = X;
-  if (ncols < nws) {
-    const int64_t tot = (int64_t)nws * ncols;
-    k_env_transpose<<<(unsigned)((tot + 255) / 256), 256, 0, st>>>(X, nws, ncols, w.B);
-    CK(cudaGetLastError());
-    A = w.B;
+// The leading r triplets: k = n_modes + 10 columns and two power iterations;
+// if that is not certified, twice the columns (up to 64 and the matrix's
+// smaller side) and four power iterations until it is.  When the columns span
+// the whole smaller side the residual is rounding only, so only n_modes above
+// 54 on a matrix wider than 64 can end uncertified: then an error.
+e2e_status truncated_svd(SvdWork& w, const double* X, int nws, int ncols, int r, const double* mean, double* C,
+                         double* M, double* svals, cudaStream_t st, int* enlarged) {
+  const int nsmall = std::min(nws, ncols);
+  int k = std::min(std::min(r + 10, kRrMaxK), nsmall), power = 2;
+  if (k < r) return fail(E2E_ERR_UNSUPPORTED, "n_modes above the range finder's 64 columns");
+  for (;;) {
+    bool ok = false;
+    e2e_status s = randomized_svd(w, X, nws, ncols, r, k, power, mean, C, M, svals, &ok, st);
+    if (s != E2E_OK) return s;
+    if (ok) return E2E_OK;
+    const int k2 = std::min(std::min(2 * k, kRrMaxK), nsmall);
+    if (k2 == k && power >= 4)
+      return fail(E2E_ERR_DEVICE, "rank reduction not certified with " + std::to_string(k) +
+                                      " columns (|X - QQ^T X| above 1e-10 s_1)");
+    ++*enlarged;
+    k = k2;
+    power = 4;
   }
-  CKS(cusolverDnDgesvdj(w.sol, CUSOLVER_EIG_MODE_VECTOR, 1, m, n, A, m, w.S, w.U, m, w.V, n, w.work, w.lwork, w.info,
-                        w.params));
-  int h_info = 0;
-  CK(cudaMemcpyAsync(&h_info, w.info, sizeof(int), cudaMemcpyDeviceToHost, st));
-  CK(cudaStreamSynchronize(st));
-  if (h_info != 0) return fail(E2E_ERR_DEVICE, "Jacobi SVD did not converge (info " + std::to_string(h_info) + ")");
-  ModeArgs a;
-  a.nws = nws;
-  a.ncols = ncols;
-  a.r = r;
-  a.S = w.S;
-  if (ncols >= nws) {  // X^T = U S V^T: sample side V (n = nws rows), grid side U (m = ncols rows)
-    a.Us = w.V;
-    a.ldu = n;
-    a.Vs = w.U;
-    a.ldv = m;
-  } else {             // X = U S V^T: sample side U (m = nws rows), grid side V (n = ncols rows)
-    a.Us = w.U;
-    a.ldu = m;
-    a.Vs = w.V;
-    a.ldv = n;
-  }
-  a.C = C;
-  a.M = M;
-  a.svals = svals;
-  k_env_modes<<<r, 256, 0, st>>>(a);
-  CK(cudaGetLastError());
-  return E2E_OK;
 }
 
 }  // namespace
@@ -594,94 +886,41 @@ extern "C" e2e_status e2e_env_generate(const e2e_env_params* p, const int32_t* i
   yi = o.yi;
   phi_yi = o.phi_yi;
 
-  // Jacobi SVD work space (the larger of the two reductions)
+  // rank-reduction work space, sized for the wider (velocity) matrix and the
+  // largest range finder
   SvdWork w;
-  struct SvdFree {
-    SvdWork* w;
-    ~SvdFree() {
-      if (w->params) cusolverDnDestroyGesvdjInfo(w->params);
-    }
-  } svdfree{&w};
-  std::unique_lock<std::mutex> handles_held;  // the device's handles, until this call returns
   {
-    e2e_status hs = solver_handles(&w.sol, &w.blas, &handles_held);
-    if (hs != E2E_OK) return hs;
-  }
-  // on every return, the work queued with the handles finishes before the
-  // next caller may set them to its own stream
-  struct DrainBeforeRelease {
-    cudaStream_t s;
-    ~DrainBeforeRelease() { cudaStreamSynchronize(s); }
-  } drain{st};
-  CKS(cusolverDnSetStream(w.sol, st));
-  CKB(cublasSetStream(w.blas, st));
-  CKB(cublasSetPointerMode(w.blas, CUBLAS_POINTER_MODE_HOST));
-  CKS(cusolverDnCreateGesvdjInfo(&w.params));
-  CKS(cusolverDnXgesvdjSetSortEig(w.params, 1));
-  {
-    size_t bu = 0, bv = 0, bs = 0, bb = 0;
-    for (int ncols : {2 * n, n}) {
-      int m, k;
-      svd_shape(nws, ncols, &m, &k);
-      bu = std::max(bu, (size_t)m * k);
-      bv = std::max(bv, (size_t)k * k);
-      bs = std::max(bs, (size_t)k);
-      if (ncols < nws) bb = std::max(bb, (size_t)nws * ncols);
-    }
-    CK(dalloc((void**)&w.U, sizeof(double) * bu, st));
-    scratch.add(w.U);
-    CK(dalloc((void**)&w.V, sizeof(double) * bv, st));
-    scratch.add(w.V);
-    CK(dalloc((void**)&w.S, sizeof(double) * bs, st));
-    scratch.add(w.S);
-    if (bb) {
-      CK(dalloc((void**)&w.B, sizeof(double) * bb, st));
-      scratch.add(w.B);
-    }
-    CK(dalloc((void**)&w.info, sizeof(int), st));
-    scratch.add(w.info);
-    for (int ncols : {2 * n, n}) {
-      int m, k, lw = 0;
-      svd_shape(nws, ncols, &m, &k);
-      CKS(cusolverDnDgesvdj_bufferSize(w.sol, CUSOLVER_EIG_MODE_VECTOR, 1, m, k, Xv, m, w.S, w.U, m, w.V, k, &lw,
-                                       w.params));
-      w.lwork = std::max(w.lwork, lw);
-    }
-    // randomized range finder: k = n_modes + 10 columns
-    w.k = std::min(r + 10, std::min(nws, n));
-    const int kk = w.k, cmax = std::max(2 * n, nws);
-    double** rb[] = {&w.Om, &w.Z, &w.Bt, &w.Ub, &w.Q, &w.L};
-    for (double** b : rb) {
-      CK(dalloc((void**)b, sizeof(double) * (size_t)cmax * kk, st));
+    w.kmax = kRrMaxK;
+    w.ncols_max = 2 * n;
+    const size_t kc = (size_t)w.ncols_max * w.kmax, ks = (size_t)nws * w.kmax, kk = (size_t)w.kmax * w.kmax;
+    double** wide[] = {&w.Om, &w.Z, &w.Bt, &w.Ub};
+    for (double** b : wide) {
+      CK(dalloc((void**)b, sizeof(double) * kc, st));
       scratch.add(*b);
     }
-    CK(dalloc((void**)&w.R, sizeof(double) * (size_t)nws * 2 * n, st));
-    scratch.add(w.R);
-    CK(dalloc((void**)&w.Vb, sizeof(double) * (size_t)kk * kk, st));
-    scratch.add(w.Vb);
-    CK(dalloc((void**)&w.Sb, sizeof(double) * (size_t)kk, st));
-    scratch.add(w.Sb);
-    CK(dalloc((void**)&w.tau, sizeof(double) * (size_t)kk, st));
-    scratch.add(w.tau);
-    for (int rows : {nws, 2 * n, n}) {
-      int lw = 0;
-      CKS(cusolverDnDgeqrf_bufferSize(w.sol, rows, kk, w.Q, rows, &lw));
-      w.lqwork = std::max(w.lqwork, lw);
-      CKS(cusolverDnDorgqr_bufferSize(w.sol, rows, kk, kk, w.Q, rows, w.tau, &lw));
-      w.lqwork = std::max(w.lqwork, lw);
+    double** tall[] = {&w.Q, &w.L};
+    for (double** b : tall) {
+      CK(dalloc((void**)b, sizeof(double) * ks, st));
+      scratch.add(*b);
     }
-    for (int ncols : {2 * n, n}) {
-      int lw = 0;
-      CKS(cusolverDnDgesvdj_bufferSize(w.sol, CUSOLVER_EIG_MODE_VECTOR, 1, ncols, kk, w.Bt, ncols, w.Sb, w.Ub,
-                                       ncols, w.Vb, kk, &lw, w.params));
-      w.lwork = std::max(w.lwork, lw);
+    double** sq[] = {&w.R, &w.V, &w.U, &w.Vs};
+    for (double** b : sq) {
+      CK(dalloc((void**)b, sizeof(double) * kk, st));
+      scratch.add(*b);
     }
-    CK(dalloc((void**)&w.qwork, sizeof(double) * (size_t)std::max(w.lqwork, 1), st));
-    scratch.add(w.qwork);
-    CK(dalloc((void**)&w.work, sizeof(double) * (size_t)std::max(w.lwork, 1), st));
-    scratch.add(w.work);
+    CK(dalloc((void**)&w.S, sizeof(double) * w.kmax, st));
+    scratch.add(w.S);
+    CK(dalloc((void**)&w.P, sizeof(double) * kRrSegs * kc, st));
+    scratch.add(w.P);
+    w.part_cap = ((w.ncols_max + 127) / 128) * kRrSegs;
+    CK(dalloc((void**)&w.part, sizeof(double) * w.part_cap, st));
+    scratch.add(w.part);
+    CK(dalloc((void**)&w.scal, sizeof(double) * 2, st));
+    scratch.add(w.scal);
+    CK(dalloc((void**)&w.sweeps, sizeof(int), st));
+    scratch.add(w.sweeps);
   }
-  int full_svds = 0;
+  int enlarged = 0;
 
   for (int t = 0; t < nt; ++t) {
     RealArgs ra{g, nws, t, (double)t * p->dt, p->dxy, p->A, p->eps, p->w_lo, p->w_hi, p->wx, 0.5 * kPi, Xv, Xp};
@@ -691,9 +930,9 @@ extern "C" e2e_status e2e_env_generate(const e2e_env_params* p, const int32_t* i
     k_env_center<<<(2 * n + 127) / 128, 128, 0, st>>>(Xv, nws, 2 * n, mv);
     k_env_center<<<(n + 127) / 128, 128, 0, st>>>(Xp, nws, n, mp);
     CK(cudaGetLastError());
-    e2e_status s = truncated_svd(w, Xv, nws, 2 * n, r, Cv, Mv, sv + (int64_t)t * r, st, &full_svds);
+    e2e_status s = truncated_svd(w, Xv, nws, 2 * n, r, mv, Cv, Mv, sv + (int64_t)t * r, st, &enlarged);
     if (s != E2E_OK) return s;
-    s = truncated_svd(w, Xp, nws, n, r, Cp, Mp, sv + (int64_t)(nt + t) * r, st, &full_svds);
+    s = truncated_svd(w, Xp, nws, n, r, mp, Cp, Mp, sv + (int64_t)(nt + t) * r, st, &enlarged);
     if (s != E2E_OK) return s;
     const int64_t ns = std::max<int64_t>((int64_t)nb * n, (int64_t)nws * r);
     k_env_store<<<(unsigned)((ns + 255) / 256), 256, 0, st>>>(n, nws, r, mv, mp, Mv, Mp, Cv, Cp,
@@ -734,9 +973,9 @@ extern "C" e2e_status e2e_env_generate(const e2e_env_params* p, const int32_t* i
     CK(cudaEventElapsedTime(&ms, ev[0], ev[1]));
     stats->seconds = ms * 1e-3;
     stats->fine_gsize = (int32_t)G;
-    stats->transposed_vel = 2 * n < nws ? 1 : 0;
-    stats->transposed_phi = n < nws ? 1 : 0;
-    stats->full_svds = full_svds;
+    stats->transposed_vel = 0;
+    stats->transposed_phi = 0;
+    stats->full_svds = enlarged;
   }
   return E2E_OK;
 }

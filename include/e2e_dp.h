@@ -408,9 +408,9 @@ typedef struct {
 typedef struct {
   double seconds;          /* device time (CUDA events) */
   int32_t fine_gsize;
-  int32_t transposed_vel;  /* 1: more samples than columns, the matrix was transposed for the SVD */
-  int32_t transposed_phi;
-  int32_t full_svds;       /* reductions that fell back from the randomized SVD to the full Jacobi SVD */
+  int32_t transposed_vel;  /* always 0 (kept for the layout: no reduction transposes its matrix) */
+  int32_t transposed_phi;  /* always 0 */
+  int32_t full_svds;       /* reductions whose range finder was re-run enlarged before it certified */
 } e2e_env_stats;
 /* interp_vertices / interp_weights: (G*G) x 3, host or device memory.
  * svals_out (may be NULL): 2 x nt x n_modes singular values (velocity, then phi). */
