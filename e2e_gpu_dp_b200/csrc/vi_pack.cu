@@ -185,11 +185,40 @@ __device__ __forceinline__ void decode(ColT o, CntT w, uint32_t& idx, float& f) 
   }
 }
 
+// The sum over a row's N slots (N = the (chunk, action) slot count, the same
+// for the whole warp): every entry load, then every gather, then the fma chain
+// in slot order.  Slots past the lane's row hold count 0 and point at a value
+// that is finite, so they add fma(0, v, acc) = acc.
+template <int N, int MODE, typename CntT, bool COHERENT>
+__device__ __forceinline__ float row_slots(const Entries<MODE, CntT>& e, const float* vb) {
+  using ColT = typename Entries<MODE, CntT>::ColT;
+  ColT o[N];
+  CntT w[N];
+#pragma unroll
+  for (int j = 0; j < N; ++j) {
+    o[j] = ld_stream(e.col + j * 32);
+    w[j] = MODE != ENT_PACKED ? ld_stream(e.cnt + j * 32) : (CntT)0;
+  }
+  float v[N], f[N];
+#pragma unroll
+  for (int j = 0; j < N; ++j) {
+    uint32_t idx;
+    decode<MODE, ColT, CntT>(o[j], w[j], idx, f[j]);
+    v[j] = ld_value<COHERENT>(vb + idx);
+  }
+  float acc = 0.f;
+#pragma unroll
+  for (int j = 0; j < N; ++j) acc = fmaf(f[j], v[j], acc);
+  return acc;
+}
+
 // Best (value, action) over actions [a0, a1) of the lane's state of chunk c;
 // the lane's R of action a is Rp[(a - a0) * rstride].  VAR 0: the next
 // action's first batch of 4 entries is loaded before this action's gathers
 // (5 CTAs per SM).  VAR 1: no look-ahead, fewer registers and 8 CTAs per SM;
-// latency is hidden by the extra warps instead.
+// latency is hidden by the extra warps instead.  VAR 2: as VAR 1, but a row of
+// up to 10 slots is one straight-line block for its exact slot count (a
+// switch on the warp-uniform count) instead of predicated batches of 4.
 template <int MODE, typename CntT, bool COHERENT, int VAR>
 __device__ __forceinline__ void chunk_best(const ViPack& P, int c, const ChunkPos& cp, int lane, int a0,
                                            int a1, const float* Vin, float& bq, int& ba,
@@ -216,6 +245,43 @@ __device__ __forceinline__ void chunk_best(const ViPack& P, int c, const ChunkPo
 #pragma unroll
     for (int j = 0; j < B; ++j) acc = fmaf(f[j], v[j], acc);
   };
+  if constexpr (VAR == 2) {
+    for (int a = a0; a < a1; ++a) {
+      const float r = ld_stream(Rp);
+      Rp += rstride;
+      const int ml = __ldg(mlp + a);
+      float acc = 0.f;
+      switch (ml) {
+        case 0: break;
+        case 1: acc = row_slots<1, MODE, CntT, COHERENT>(cur, vb); break;
+        case 2: acc = row_slots<2, MODE, CntT, COHERENT>(cur, vb); break;
+        case 3: acc = row_slots<3, MODE, CntT, COHERENT>(cur, vb); break;
+        case 4: acc = row_slots<4, MODE, CntT, COHERENT>(cur, vb); break;
+        case 5: acc = row_slots<5, MODE, CntT, COHERENT>(cur, vb); break;
+        case 6: acc = row_slots<6, MODE, CntT, COHERENT>(cur, vb); break;
+        case 7: acc = row_slots<7, MODE, CntT, COHERENT>(cur, vb); break;
+        case 8: acc = row_slots<8, MODE, CntT, COHERENT>(cur, vb); break;
+        case 9: acc = row_slots<9, MODE, CntT, COHERENT>(cur, vb); break;
+        case 10: acc = row_slots<10, MODE, CntT, COHERENT>(cur, vb); break;
+        default:
+          for (int k0 = 0; k0 < ml; k0 += B) {
+            E more = cur;
+            more.advance(k0);
+            ColT o2[B];
+            CntT w2[B];
+            more.template load<B>(min(ml - k0, B), o2, w2);
+            fold(o2, w2, min(ml - k0, B), acc);
+          }
+      }
+      const float q = finish_row(r, acc, 0.f, P.nrzns, counts);
+      if (!isnan(q) && q > bq) {
+        bq = q;
+        ba = a;
+      }
+      cur.advance(ml);
+    }
+    return;
+  }
   int ml = a0 < a1 ? __ldg(mlp + a0) : 0;
   ColT o[B];
   CntT w[B];
@@ -654,7 +720,8 @@ __global__ void __launch_bounds__(kThreads, MinBlocks<MODE, VAR>::value)
 // nrzns) and R = 0, evaluated here with the same operations as that row.
 template <int MODE, int VAR>
 struct BatchMinBlocks {  // the job lookup needs a few more registers than k_vi_layered (lean: 6 CTAs
-                        // per SM measured 24.1 ms on the 256-model batch, 5: 24.7, 8: 25.5)
+                        // per SM measured 24.1 ms on the 256-model batch, 5: 24.7, 8: 25.5; with
+                        // exact-count rows 22.3 ms)
   static constexpr int value = MODE != ENT_PACKED ? 3 : (VAR == 0 ? 4 : 6);
 };
 
@@ -1062,7 +1129,7 @@ cudaError_t launch_vi_chunks(const ViPack& P, int64_t c_begin, int64_t c_end, co
     using CntT = std::remove_pointer_t<decltype(cntt)>;
     constexpr int MODE = decltype(mode)::value;
     const bool lean = MODE == ENT_PACKED && (tune & VI_TUNE_LEAN);
-    auto kern = lean ? k_vi_chunks<MODE, CntT, (MODE == ENT_PACKED ? 1 : 0)> : k_vi_chunks<MODE, CntT, 0>;
+    auto kern = lean ? k_vi_chunks<MODE, CntT, (MODE == ENT_PACKED ? 2 : 0)> : k_vi_chunks<MODE, CntT, 0>;
     const int64_t need = (c_end - c_begin + kWarps - 1) / kWarps;
     const int64_t cap = (int64_t)occupancy((const void*)kern) * sm_count_pack();
     const unsigned grid = (unsigned)std::min(need, cap);
@@ -1078,7 +1145,7 @@ cudaError_t launch_vi_layered(const ViPack& P, float* V, int32_t* pi, unsigned i
     using CntT = std::remove_pointer_t<decltype(cntt)>;
     constexpr int MODE = decltype(mode)::value;
     const bool lean = MODE == ENT_PACKED && (tune & VI_TUNE_LEAN);
-    auto kern = lean ? k_vi_layered<MODE, CntT, (MODE == ENT_PACKED ? 1 : 0)> : k_vi_layered<MODE, CntT, 0>;
+    auto kern = lean ? k_vi_layered<MODE, CntT, (MODE == ENT_PACKED ? 2 : 0)> : k_vi_layered<MODE, CntT, 0>;
     const int64_t cap = (int64_t)occupancy((const void*)kern) * sm_count_pack();
     int G = groups;
     if (G <= 0) {
@@ -1123,7 +1190,7 @@ int vi_batch_capacity(int ent_mode, int count_type, int tune) {
     using CntT = std::remove_pointer_t<decltype(cntt)>;
     constexpr int MODE = decltype(mode)::value;
     const bool lean = MODE == ENT_PACKED && (tune & VI_TUNE_LEAN);
-    auto kern = lean ? k_vi_batch<MODE, CntT, (MODE == ENT_PACKED ? 1 : 0)> : k_vi_batch<MODE, CntT, 0>;
+    auto kern = lean ? k_vi_batch<MODE, CntT, (MODE == ENT_PACKED ? 2 : 0)> : k_vi_batch<MODE, CntT, 0>;
     cap = occupancy((const void*)kern) * sm_count_pack();
     return cudaSuccess;
   });
@@ -1138,7 +1205,7 @@ cudaError_t launch_vi_batch(const void* table, int job_cap, int layer_cap, int e
     using CntT = std::remove_pointer_t<decltype(cntt)>;
     constexpr int MODE = decltype(mode)::value;
     const bool lean = MODE == ENT_PACKED && (tune & VI_TUNE_LEAN);
-    auto kern = lean ? k_vi_batch<MODE, CntT, (MODE == ENT_PACKED ? 1 : 0)> : k_vi_batch<MODE, CntT, 0>;
+    auto kern = lean ? k_vi_batch<MODE, CntT, (MODE == ENT_PACKED ? 2 : 0)> : k_vi_batch<MODE, CntT, 0>;
     const int cap = occupancy((const void*)kern) * sm_count_pack();
     if (grid < 1 || grid > cap) return cudaErrorInvalidValue;  // CTAs must be co-resident
     cudaLaunchConfig_t cfg{};
