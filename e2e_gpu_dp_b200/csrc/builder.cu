@@ -23,6 +23,7 @@
 //    one atomicAdd per CTA, with the row's tile-relative offset and R = sumR/nrzns;
 //  * K2 scans the tile lengths, K3 moves every tile into canonical CSR order and
 //    writes row_ptr.
+#include <algorithm>
 #include <mutex>
 
 #include "common.cuh"
@@ -85,8 +86,7 @@ __device__ __forceinline__ void fused_backup(const BuildArgs& A, int T, int64_t 
   const DevProblem& P = A.P;
   const int g = P.g;
   const int64_t nc = (int64_t)g * g;
-  // values of layer T+1 are complete once the previous launch has completed
-  asm volatile("griddepcontrol.wait;" ::: "memory");
+  // the caller waited for the rows of layer T+1 that it reads (wait_rows)
   const float* Vn = A.V + (int64_t)(T + 1) * nc;
   float acc = 0.f;
   int nnz = 0;
@@ -218,9 +218,49 @@ __device__ __forceinline__ void vel_pairs4(const float2* md, const float* y0, in
   }
 }
 
+// Fused build+backup: warp 0 waits until every cell of rows lo..hi of layer
+// `layer` is backed up (per (layer, grid row) completion counters, released
+// by the CTAs of those cells), then the CTA passes a barrier, so every
+// thread's later loads of those values are ordered after the writes.  The
+// wait is bounded: past A.wait_ns (or a poll limit) it sets FLAG_WAIT_TIMEOUT
+// and returns, and once the flag is set every later wait returns at once, so
+// the launch drains.  The last layer has no rows: its values are written
+// before the launch.
+__device__ __forceinline__ void wait_rows(const BuildArgs& A, int layer, int lo, int hi) {
+  if (threadIdx.x < 32 && layer <= A.P.nt - 2) {
+    const int lane = threadIdx.x;
+    const unsigned int target = (unsigned int)A.P.g + A.wait_extra;
+    const unsigned int* done = A.layer_done + (int64_t)layer * A.P.g;
+    unsigned int* flags = reinterpret_cast<unsigned int*>(A.counters + CTR_FLAGS);
+    unsigned long long t0;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t0));
+    long long it = 0;
+    for (;;) {
+      bool ok = true;
+      for (int r = lo + lane; r <= hi; r += 32) {
+        unsigned int v;
+        asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(done + r) : "memory");
+        ok = ok && v >= target;
+      }
+      if (__all_sync(0xffffffffu, ok)) break;
+      unsigned int f;
+      asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(f) : "l"(flags) : "memory");
+      unsigned long long t;
+      asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+      const bool give_up = (f & FLAG_WAIT_TIMEOUT) || ++it > (1ll << 26) || t - t0 > A.wait_ns;
+      if (__any_sync(0xffffffffu, give_up)) {
+        if (lane == 0) atomicOr(flags, FLAG_WAIT_TIMEOUT);
+        break;
+      }
+      __nanosleep(64);
+    }
+  }
+  __syncthreads();
+}
+
+// K1 on one tile (32 cells of layer T and all their actions) by one CTA.
 template <typename CntT, bool UNIT, bool FUSED>
-__global__ void __launch_bounds__(1024) k_build_tiles(BuildArgs A) {
-  extern __shared__ __align__(16) unsigned char smem[];
+__device__ __forceinline__ void build_tile(const BuildArgs& A, unsigned char* smem, const int T, const int tile) {
   const DevProblem& P = A.P;
   const int nthr = blockDim.x;
   const int tid = threadIdx.x;
@@ -231,10 +271,9 @@ __global__ void __launch_bounds__(1024) k_build_tiles(BuildArgs A) {
   const int a = lane & ((1 << lanes_log2) - 1);  // action of this lane
   const int cw = lane >> lanes_log2;             // cell within warp
   const int cl = warp * (32 >> lanes_log2) + cw; // cell within tile (0..31)
-  const int T = A.t0 + blockIdx.y;
   const int g = P.g;
   const int64_t nc = (int64_t)g * g;
-  const int64_t c0 = (int64_t)blockIdx.x * 32;
+  const int64_t c0 = (int64_t)tile * 32;
   const int64_t cell = c0 + cl;
   const bool valid = (cell < nc) && (a < P.na);
   const int nm = P.nm;
@@ -253,10 +292,6 @@ __global__ void __launch_bounds__(1024) k_build_tiles(BuildArgs A) {
   uint16_t* const wcol = win + counter_col(warp, lane);
   float* const ysm = reinterpret_cast<float*>(win + ((size_t)(kWinBins + 1) << log2S));  // rc x coeff_stride(nm)
 
-  // the next layer's launch may start its CTAs once every CTA of this one has
-  // started (programmatic dependent launch); it reads this layer's values only
-  // after griddepcontrol.wait, i.e. after this grid has completed
-  if (FUSED) asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
 
   // ---- stage the modes of the tile's cells as (ui_k, vi_k) pairs ---------
   for (int idx = tid; idx < 2 * nm * 32; idx += nthr) {
@@ -804,8 +839,23 @@ __global__ void __launch_bounds__(1024) k_build_tiles(BuildArgs A) {
   if (mode == MODE_LOST) atomicOr(reinterpret_cast<unsigned int*>(A.counters + CTR_FLAGS), FLAG_POOL_EXHAUSTED);
 
   if (FUSED) {
+    // the backup reads layer T+1 within the rows' m x m neighbourhoods and
+    // 8 x 8 windows: rows of the tile's cells +- max(del, 7)
+    const int64_t c_last = min(c0 + 31, nc - 1);
+    const int r0 = (int)(c0 / g), r1 = (int)(c_last / g), reach = max(P.del, kWin - 1);
+    wait_rows(A, T + 1, max(r0 - reach, 0), min(r1 + reach, g - 1));
     fused_backup(A, T, cell, valid, cvalid, a, lane, lanes_log2, mode, sumR, wcol, log2S, wi0, wj0, i1, j1,
                  dense);
+    __syncthreads();  // every row of the tile is backed up
+    if (tid == 0) {
+      __threadfence();
+      for (int r = r0; r <= r1; ++r) {  // the tile's cells in each grid row it spans
+        const int64_t lo = max(c0, (int64_t)r * g), hi = min(c_last, (int64_t)(r + 1) * g - 1);
+        asm volatile("red.release.gpu.global.add.u32 [%0], %1;" ::"l"(A.layer_done + (int64_t)T * g + r),
+                     "r"((unsigned int)(hi - lo + 1))
+                     : "memory");
+      }
+    }
     return;
   }
 
@@ -831,9 +881,9 @@ __global__ void __launch_bounds__(1024) k_build_tiles(BuildArgs A) {
   unsigned long long wbase = 0;
   if (lane == 0) {
     wbase = atomicAdd(A.counters + CTR_STAGE, (unsigned long long)total);
-    const int64_t tile = ((int64_t)T * A.tiles_per_layer + blockIdx.x) * nwarps + warp;
-    A.tile_base[tile] = (int64_t)wbase;
-    A.tile_len[tile] = total;
+    const int64_t wt = ((int64_t)T * A.tiles_per_layer + tile) * nwarps + warp;
+    A.tile_base[wt] = (int64_t)wbase;
+    A.tile_len[wt] = total;
   }
   wbase = __shfl_sync(0xffffffffu, wbase, 0);
   if (!valid) return;
@@ -870,6 +920,44 @@ __global__ void __launch_bounds__(1024) k_build_tiles(BuildArgs A) {
         ++off;
       }
     }
+  }
+}
+
+// K1 over a grid of (tile, layer - t0) CTAs.
+template <typename CntT, bool UNIT>
+__global__ void __launch_bounds__(1024) k_build_tiles(BuildArgs A) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  build_tile<CntT, UNIT, false>(A, smem, A.t0 + (int)blockIdx.y, (int)blockIdx.x);
+}
+
+// Fused build+backup of all layers in one cooperative launch.  Tiles are
+// numbered g = 0, 1, ... with layer nt-2-g/tiles_per_layer, and a CTA that is
+// ready takes the next number from a counter (CTR_NEXT_TILE); a tile samples,
+// waits for the layer after its own (wait_rows), backs its rows up and counts
+// itself done.  Every tile of layer t+1 has a smaller number than every tile
+// of layer t and numbers are taken in increasing order by resident CTAs (a
+// cooperative launch), so by induction over g every awaited tile has been
+// taken and finishes: the waits end.  A tile waits only for the rows of layer
+// t+1 its backup reads (its cells' rows +- max(del, 7)), which were taken
+// about a layer's worth of tiles before it.  Sampling needs no values, so a
+// layer's sampling overlaps the completion of the layer after it, with no
+// launch boundary between layers.  (Fixed assignment, CTA b taking g = b, b + grid,
+// ..., let slow CTAs fall ever further behind and the others wait for them at
+// every layer: 400 ms on c2 against 367 ms with one launch per layer.)
+template <typename CntT, bool UNIT>
+__global__ void __launch_bounds__(1024) k_build_fused(BuildArgs A) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  __shared__ long long taken;
+  const int64_t tpl = A.tiles_per_layer;
+  const int64_t total = (int64_t)(A.P.nt - 1) * tpl;
+  for (;;) {
+    if (threadIdx.x == 0) taken = (long long)atomicAdd(A.counters + CTR_NEXT_TILE, 1ull);
+    __syncthreads();
+    const int64_t g = taken;
+    if (g >= total) break;
+    const int L = (int)(g / tpl);
+    build_tile<CntT, UNIT, true>(A, smem, A.P.nt - 2 - L, (int)(g - (int64_t)L * tpl));
+    __syncthreads();  // the next tile reuses the shared memory (and `taken`)
   }
 }
 
@@ -1001,44 +1089,55 @@ size_t build_smem_bytes(int na, int nm, int rc, bool unit) {
          (size_t)rc * coeff_stride(nm) * sizeof(float);
 }
 
-template <typename CntT, bool UNIT, bool FUSED = false>
+// the dynamic shared-memory cap of a kernel only grows: builds on other host
+// threads may be launching it with a larger need at the same time
+template <typename K>
+static cudaError_t raise_smem_cap(K kern, size_t sm, int* cap_set, std::mutex& mu) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  std::lock_guard<std::mutex> lk(mu);
+  if (dev >= 0 && dev < 64 && (int)sm > cap_set[dev]) {
+    e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    if (e != cudaSuccess) return e;
+    cap_set[dev] = (int)sm;
+  }
+  return cudaSuccess;
+}
+
+template <typename CntT, bool UNIT>
 static cudaError_t launch_one(const BuildArgs& A, int n_layers, cudaStream_t st) {
   dim3 grid((unsigned)A.tiles_per_layer, (unsigned)n_layers);
   dim3 block((unsigned)(32u << A.lanes_log2));
-  size_t sm = build_smem_bytes(A.P.na, A.P.nm, A.rc, UNIT);
-  {
-    // the shared-memory cap only grows: builds on other host threads may be
-    // launching this kernel with a larger need at the same time
-    static std::mutex mu;
-    static int cap_set[64] = {};
-    int dev = 0;
-    cudaError_t e = cudaGetDevice(&dev);
-    if (e != cudaSuccess) return e;
-    std::lock_guard<std::mutex> lk(mu);
-    if (dev >= 0 && dev < 64 && (int)sm > cap_set[dev]) {
-      e = cudaFuncSetAttribute(k_build_tiles<CntT, UNIT, FUSED>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                               (int)sm);
-      if (e != cudaSuccess) return e;
-      cap_set[dev] = (int)sm;
-    }
-  }
-  if (!FUSED) {
-    k_build_tiles<CntT, UNIT, FUSED><<<grid, block, sm, st>>>(A);
-    return cudaGetLastError();
-  }
-  // programmatic dependent launch: this layer's CTAs start while the previous
-  // layer's last CTAs finish; griddepcontrol.wait orders the reads of its values
-  cudaLaunchConfig_t cfg{};
-  cfg.gridDim = grid;
-  cfg.blockDim = block;
-  cfg.dynamicSmemBytes = sm;
-  cfg.stream = st;
-  cudaLaunchAttribute attr[1];
-  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
-  attr[0].val.programmaticStreamSerializationAllowed = 1;
-  cfg.attrs = attr;
-  cfg.numAttrs = 1;
-  return cudaLaunchKernelEx(&cfg, k_build_tiles<CntT, UNIT, FUSED>, A);
+  const size_t sm = build_smem_bytes(A.P.na, A.P.nm, A.rc, UNIT);
+  static std::mutex mu;
+  static int cap_set[64] = {};
+  cudaError_t e = raise_smem_cap(k_build_tiles<CntT, UNIT>, sm, cap_set, mu);
+  if (e != cudaSuccess) return e;
+  k_build_tiles<CntT, UNIT><<<grid, block, sm, st>>>(A);
+  return cudaGetLastError();
+}
+
+template <bool UNIT>
+static cudaError_t launch_fused(const BuildArgs& A, cudaStream_t st, int* grid_out) {
+  auto kern = k_build_fused<uint32_t, UNIT>;
+  const int threads = 32 << A.lanes_log2;
+  const size_t sm = build_smem_bytes(A.P.na, A.P.nm, A.rc, UNIT);
+  static std::mutex mu;
+  static int cap_set[64] = {};
+  cudaError_t e = raise_smem_cap(kern, sm, cap_set, mu);
+  if (e != cudaSuccess) return e;
+  int dev = 0, per_sm = 0, sms = 0;
+  if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;
+  if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
+  if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, sm)) != cudaSuccess) return e;
+  if (per_sm < 1) return cudaErrorInvalidConfiguration;
+  const int64_t total = (int64_t)(A.P.nt - 1) * A.tiles_per_layer;
+  const unsigned grid = (unsigned)std::max<int64_t>(1, std::min<int64_t>(total, (int64_t)per_sm * sms));
+  if (grid_out) *grid_out = (int)grid;
+  BuildArgs B = A;
+  void* args[] = {&B};
+  return cudaLaunchCooperativeKernel((const void*)kern, dim3(grid), dim3((unsigned)threads), args, sm, st);
 }
 
 cudaError_t launch_build_tiles(const BuildArgs& A, int count_bits, int n_layers,
@@ -1049,10 +1148,8 @@ cudaError_t launch_build_tiles(const BuildArgs& A, int count_bits, int n_layers,
   return unit ? launch_one<uint32_t, true>(A, n_layers, st) : launch_one<uint32_t, false>(A, n_layers, st);
 }
 
-cudaError_t launch_build_fused(const BuildArgs& A, int layer, cudaStream_t st) {
-  BuildArgs B = A;
-  B.t0 = layer;
-  return A.P.unit_step != 0 ? launch_one<uint32_t, true, true>(B, 1, st) : launch_one<uint32_t, false, true>(B, 1, st);
+cudaError_t launch_build_fused(const BuildArgs& A, cudaStream_t st, int* grid) {
+  return A.P.unit_step != 0 ? launch_fused<true>(A, st, grid) : launch_fused<false>(A, st, grid);
 }
 
 cudaError_t launch_scan_tiles(const int32_t* tile_len, int64_t n_tiles, int64_t* canon,

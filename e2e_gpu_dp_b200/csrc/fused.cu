@@ -7,12 +7,14 @@
 // values of layer t are final as soon as layer t+1's are: the layered schedule
 // reaches the Jacobi fixed point in one pass.  Here each layer's rows are built
 // by K1 and backed up in its epilogue from the counters still in shared memory
-// (launch_build_fused), layers nt-2 down to 0, one launch each on one stream
-// with programmatic dependent launch so that a layer's sampling overlaps the
-// previous layer's last CTAs.
+// (launch_build_fused): one cooperative launch whose CTAs take the tiles of
+// layers nt-2 down to 0 in order, each tile waiting (bounded) before its
+// backup only for the rows of the layer after its own that the backup reads,
+// so a layer's sampling overlaps the completion of the next one.
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cstdlib>
 
 #include "e2e_dp.h"
 #include "internal.h"
@@ -72,6 +74,20 @@ extern "C" e2e_status e2e_build_solve(const e2e_problem* p, const e2e_fields* f,
   unsigned long long* ctr = nullptr;
   CK(dalloc((void**)&ctr, sizeof(unsigned long long) * CTR_COUNT, st));
   scratch.add(ctr);
+  unsigned int* done = nullptr;  // per (layer, grid row): cells backed up
+  const size_t n_done = (size_t)p->nt * (size_t)p->gsize;
+  CK(dalloc((void**)&done, sizeof(unsigned int) * n_done, st));
+  scratch.add(done);
+  // bound of one wait for a layer's completion: E2E_WAIT_LIMIT_MS (default
+  // 5000); E2E_TEST_UNREACHABLE_WAIT=1 raises the targets so that none
+  // completes (tests of the bounded waits only)
+  unsigned long long wait_ns = 5000000000ull;
+  if (const char* ms = std::getenv("E2E_WAIT_LIMIT_MS")) {
+    const double v = std::atof(ms);
+    if (v > 0 && v <= 60000) wait_ns = (unsigned long long)(v * 1e6);
+  }
+  const char* unreachable = std::getenv("E2E_TEST_UNREACHABLE_WAIT");
+  const unsigned int wait_extra = (unreachable && unreachable[0] == '1') ? 1u : 0u;
   const int mm = p->neighb_gsize * p->neighb_gsize;
   int64_t pool_units = pl.pool_units;
   uint32_t* pool = nullptr;
@@ -86,6 +102,7 @@ extern "C" e2e_status e2e_build_solve(const e2e_problem* p, const e2e_fields* f,
   for (int attempt = 0; attempt < 3; ++attempt) {
     if (!pool) CK(dalloc((void**)&pool, sizeof(uint32_t) * (size_t)mm * (size_t)pool_units, st));
     CK(cudaMemsetAsync(ctr, 0, sizeof(unsigned long long) * CTR_COUNT, st));
+    CK(cudaMemsetAsync(done, 0, sizeof(unsigned int) * n_done, st));
     BuildArgs A{};
     A.P = D;
     A.F = fd.F;
@@ -97,9 +114,13 @@ extern "C" e2e_status e2e_build_solve(const e2e_problem* p, const e2e_fields* f,
     A.pool_units = pool_units;
     A.V = dV;
     A.pi = dpi;
+    A.layer_done = done;
+    A.wait_ns = wait_ns;
+    A.wait_extra = wait_extra;
     CK(cudaEventRecord(ev[0], st));
-    for (int t = p->nt - 2; t >= 0; --t) {
-      CK(launch_build_fused(A, t, st));
+    if (p->nt > 1) {
+      int grid = 0;
+      CK(launch_build_fused(A, st, &grid));
       ++launches;
     }
     CK(cudaEventRecord(ev[1], st));
@@ -107,6 +128,8 @@ extern "C" e2e_status e2e_build_solve(const e2e_problem* p, const e2e_fields* f,
     CK(sleep_sync(st));
     CK(cudaMemcpyAsync(hc, ctr, sizeof(hc), cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
+    if (hc[CTR_FLAGS] & FLAG_WAIT_TIMEOUT)
+      return fail(E2E_ERR_DEVICE, "fused build+backup: a wait for a layer's completion ran out of its bound");
     if (!(hc[CTR_FLAGS] & FLAG_POOL_EXHAUSTED)) break;
     // rows that found no dense histogram were not backed up: again with the
     // pool size the pass asked for

@@ -17,9 +17,12 @@ enum : int {
   CTR_OVERFLOW_ROWS = 3,  // rows that left the fast window
   CTR_POOL = 4,           // dense-histogram pool slots requested
   CTR_FLAGS = 5,          // error flags
+  CTR_NEXT_TILE = 6,      // fused build+backup: the next tile to take
   CTR_COUNT = 8
 };
-enum : unsigned int { FLAG_POOL_EXHAUSTED = 1u };
+// FLAG_WAIT_TIMEOUT: a wait of the fused build+backup for the next layer's
+// completion ran out of its bound (the pass's values are not valid)
+enum : unsigned int { FLAG_POOL_EXHAUSTED = 1u, FLAG_WAIT_TIMEOUT = 2u };
 
 struct BuildArgs {
   DevProblem P;
@@ -41,6 +44,9 @@ struct BuildArgs {
   int64_t pool_units;
   float* V;                      // fused build+backup: values (ns), layer t+1 read, layer t written
   int32_t* pi;                   // fused build+backup: policy (ns)
+  unsigned int* layer_done;      // fused build+backup: per (layer, grid row), cells backed up (nt x g, zeroed per pass)
+  unsigned long long wait_ns;    // fused build+backup: bound of a wait for a layer's completion
+  unsigned int wait_extra;       // test hook: raises the waits' targets so that none completes
 };
 
 struct AssembleArgs {
@@ -60,9 +66,11 @@ struct AssembleArgs {
 int build_lanes_log2(int na);
 size_t build_smem_bytes(int na, int nm, int rc, bool unit);
 cudaError_t launch_build_tiles(const BuildArgs& A, int count_bits, int n_layers, cudaStream_t st);
-// One layer of the fused build+backup (uses A.V, A.pi, A.pool, A.counters;
-// no staging): launched for layers nt-2 down to 0 on one stream.
-cudaError_t launch_build_fused(const BuildArgs& A, int layer, cudaStream_t st);
+// The fused build+backup of every layer (uses A.V, A.pi, A.pool, A.counters,
+// A.layer_done; no staging): one cooperative launch whose CTAs take the tiles
+// of layers nt-2 down to 0 in order and back each row up as soon as layer t+1
+// is complete.  *grid receives the CTAs launched.
+cudaError_t launch_build_fused(const BuildArgs& A, cudaStream_t st, int* grid);
 cudaError_t launch_scan_tiles(const int32_t* tile_len, int64_t n_tiles, int64_t* canon,
                               int64_t* total, int64_t* block_sums, cudaStream_t st);
 cudaError_t launch_assemble(const AssembleArgs& A, int count_bits, int index_bits,

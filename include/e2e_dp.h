@@ -360,15 +360,17 @@ e2e_status e2e_rollout(const e2e_problem* p, const e2e_fields* f, int fields_whe
  * fields, V and policy).  Value and policy are bit-identical to
  * e2e_build_model + e2e_spvi_solve with the layered method (whose fixed point
  * is the Jacobi one); last layer: value 0, action 0.  policy_out / value_out:
- * ns entries each in out_where memory (either may be NULL). */
+ * ns entries each in out_where memory (either may be NULL).  One cooperative
+ * launch: a tile's backup waits (bounded by E2E_WAIT_LIMIT_MS, default 5000)
+ * for the next layer's completion; a wait that runs out gives E2E_ERR_DEVICE. */
 typedef struct {
-  double seconds;          /* device time of the per-layer launches (CUDA events) */
+  double seconds;          /* device time of the pass (CUDA events) */
   int64_t n_rows;          /* rows built and backed up */
   int64_t nnz;             /* entries backed up (the model's nnz) */
   uint64_t dropped;        /* as e2e_model_info */
   uint64_t misbinned;
   uint64_t overflow_rows;
-  int32_t launches;        /* kernel launches (nt - 1 per pass; a pass is re-run when rows needed more dense histograms) */
+  int32_t launches;        /* kernel launches (one cooperative launch per pass; a pass is re-run when rows needed more dense histograms) */
   int32_t reserved;
   int64_t h2d_bytes;       /* field bytes copied from host memory */
 } e2e_fused_stats;

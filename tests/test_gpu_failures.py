@@ -1,7 +1,8 @@
 """Failure paths on the GPU, in the forms that fault nothing.
 
-* Bounded device waits: the persistent layered sweep waits on grid barriers
-  and the batched sweep on per-layer completion counters; every wait gives up
+* Bounded device waits: the persistent layered sweep waits on grid barriers,
+  the batched sweep and the fused build+backup on per-layer completion
+  counters; every wait gives up
   after a limit, sets an error word and lets the launch drain, and the host
   returns E2E_ERR_DEVICE.  The test hook E2E_TEST_UNREACHABLE_WAIT=1 raises
   every wait's target by one so that no wait can complete, with the limit cut
@@ -73,6 +74,19 @@ def test_batched_completion_wait_runs_out(model):
     api.solve_batch([m], [Vd], [pid], schedule=sch)
     torch.cuda.synchronize()
     assert np.array_equal(Vd.cpu().numpy(), V) and np.array_equal(pid.cpu().numpy(), pi)
+
+
+def test_fused_layer_wait_runs_out(model):
+    prob, m, V, pi = model
+    _, fields = problem("t_custom")
+    t0 = time.time()
+    with _UnreachableWaits():
+        with pytest.raises(E2EError) as ei:
+            api.build_solve(prob, fields)
+    assert ei.value.status == E2E_ERR_DEVICE
+    assert time.time() - t0 < 30
+    Vf, pif = api.build_solve(prob, fields)[:2]  # the context is still usable
+    assert np.array_equal(Vf, V) and np.array_equal(pif, pi)
 
 
 def test_jacobi_wall_clock_limit(model):

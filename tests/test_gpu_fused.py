@@ -42,7 +42,7 @@ def test_fused_equals_build_then_layered_solve(solved, name):
     assert st["n_rows"] == info["n_rows"]
     assert st["nnz"] == info["nnz"]
     assert st["dropped"] == info["dropped"] and st["overflow_rows"] == info["overflow_units"]
-    assert st["launches"] >= prob.nt - 1
+    assert st["launches"] >= 1  # one cooperative launch per pass (a pass re-runs for a larger pool)
 
 
 def test_fused_dense_rows_are_backed_up(solved):
