@@ -182,7 +182,10 @@ e2e_status e2e_action_table(const e2e_problem* p, float* speed, float* angle, fl
                             float* sinv);
 
 /* ---- build (replaces build_model main, src/build_model.cu:926-1238, and the
- * per-(t,a) worker build_sparse_transition_model_at_T_at_a, :696-892) -------- */
+ * per-(t,a) worker build_sparse_transition_model_at_T_at_a, :696-892) --------
+ * Limit the reference does not have: nrzns <= 32767 (a row's window counters
+ * are 16 bits, bit 15 marking an obstacle-overridden bin); above it the call
+ * returns E2E_ERR_UNSUPPORTED.  The same holds for e2e_build_solve. */
 e2e_status e2e_build_model(const e2e_problem* p, const e2e_fields* fields, int fields_where,
                            const e2e_build_opts* opts /* may be NULL */, e2e_model** out,
                            void* stream);
