@@ -36,7 +36,7 @@
 namespace e2e {
 namespace {
 
-constexpr int kJobCap = 1024;
+constexpr int kJobCap = kViBatchJobCap;
 constexpr int kLayerCap = 4096;
 
 struct Choice {

@@ -175,6 +175,7 @@ struct ViBatchHeader {
 // on layer nlayers-1-k of jobs [0, nact[k]): chunk items [0, cum[nact[k]]),
 // each waiting only for its own job's next layer.
 size_t vi_batch_table_bytes(int job_cap, int layer_cap);
+constexpr int kViBatchJobCap = 1024;  // jobs of one batched launch at most
 constexpr size_t kViBatchJobsOffset = 64;  // header padded to 64 bytes
 // CTAs of the batch kernel that fit on the device at once
 int vi_batch_capacity(int ent_mode, int count_type, int tune);

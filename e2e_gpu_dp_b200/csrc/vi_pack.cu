@@ -731,10 +731,16 @@ __global__ void __launch_bounds__(kThreads, BatchMinBlocks<MODE, VAR>::value)
                unsigned int* err, int prefetch, WaitBound wb) {
   __shared__ float sq[kWarps][32];
   __shared__ int sa[kWarps][32];
+  // the jobs' chunk prefix sums, the same at every step (a step uses a prefix
+  // of the jobs): searched in shared memory for every item instead of through
+  // eight dependent global loads (batched sweep of 256 models 22.1 -> 21.1 ms)
+  __shared__ int cum[kViBatchJobCap + 1];
   const ViBatchHeader* H = reinterpret_cast<const ViBatchHeader*>(table);
   const ViJob* jobs = reinterpret_cast<const ViJob*>(table + kViBatchJobsOffset);
-  const int* cum = reinterpret_cast<const int*>(jobs + job_cap);
-  const int* nact = cum + job_cap + 1;
+  const int* gcum = reinterpret_cast<const int*>(jobs + job_cap);
+  const int* nact = gcum + job_cap + 1;
+  for (int i = threadIdx.x; i <= H->njobs; i += blockDim.x) cum[i] = gcum[i];
+  __syncthreads();
   const int L = H->max_layers;
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   const int cpc = kWarps / groups;
@@ -757,7 +763,7 @@ __global__ void __launch_bounds__(kThreads, BatchMinBlocks<MODE, VAR>::value)
         int lo = 0, hi = nj - 1;  // last job with cum[job] <= item
         while (lo < hi) {
           const int mid = (lo + hi + 1) >> 1;
-          if (__ldg(cum + mid) <= item) lo = mid;
+          if (cum[mid] <= item) lo = mid;
           else hi = mid - 1;
         }
         const ViJob& J = jobs[lo];
@@ -768,7 +774,7 @@ __global__ void __launch_bounds__(kThreads, BatchMinBlocks<MODE, VAR>::value)
         const int a1 = min(na, a0 + apg);
         const int cpl = (int)P.cpl, nc = (int)P.nc;
         const int t = P.nlayers - 1 - k;
-        const int c = t * cpl + (item - __ldg(cum + lo));
+        const int c = t * cpl + (item - cum[lo]);
         done_slot = done + (int64_t)lo * layer_cap + t;
         if ((prefetch & PF_NEXT) && lane == 0 && grp == 0 && t > 0)
           prefetch_chunk(P, c - cpl, Widths<MODE, CntT>::col, Widths<MODE, CntT>::cnt);
@@ -1200,6 +1206,7 @@ int vi_batch_capacity(int ent_mode, int count_type, int tune) {
 cudaError_t launch_vi_batch(const void* table, int job_cap, int layer_cap, int ent_mode, int count_type,
                             int groups, int grid, int tune, int* done, unsigned int* err, cudaStream_t st) {
   if (groups != 1 && groups != 2 && groups != 4 && groups != 8) return cudaErrorInvalidValue;
+  if (job_cap > kViBatchJobCap) return cudaErrorInvalidValue;  // the kernel's shared prefix sums
   const int prefetch = tune & (PF_NEXT | PF_CURRENT);
   return dispatch_key(PackKey{ent_mode, count_type}, [&](auto mode, auto* cntt) -> cudaError_t {
     using CntT = std::remove_pointer_t<decltype(cntt)>;
