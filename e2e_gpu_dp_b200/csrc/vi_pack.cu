@@ -719,10 +719,11 @@ __global__ void __launch_bounds__(kThreads, MinBlocks<MODE, VAR>::value)
 // (src/build_model.cu:523-545), i.e. one entry (the cell at t+1, count
 // nrzns) and R = 0, evaluated here with the same operations as that row.
 template <int MODE, int VAR>
-struct BatchMinBlocks {  // the job lookup needs a few more registers than k_vi_layered (lean: 6 CTAs
-                        // per SM measured 24.1 ms on the 256-model batch, 5: 24.7, 8: 25.5; with
-                        // exact-count rows 22.3 ms)
-  static constexpr int value = MODE != ENT_PACKED ? 3 : (VAR == 0 ? 4 : 6);
+struct BatchMinBlocks {  // the job lookup needs more registers than k_vi_layered (lean, batches of 4:
+                        // 6 CTAs per SM measured 24.1 ms on the 256-model batch, 5: 24.7, 8: 25.5;
+                        // with exact-count rows and the prefix sums in shared memory 6 CTAs 21.1 ms,
+                        // 5 CTAs 19.9 ms, and 3.8 against 4.2 ms for one 300x300x150 job)
+  static constexpr int value = MODE != ENT_PACKED ? 3 : (VAR == 0 ? 4 : 5);
 };
 
 template <int MODE, typename CntT, int VAR>
