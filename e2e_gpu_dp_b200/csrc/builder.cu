@@ -157,9 +157,10 @@ __device__ __forceinline__ void fused_backup(const BuildArgs& A, int T, int64_t 
 // the full reference expression for it afterwards, so its reward joins the
 // row's sum after the chunk's in-window rewards.
 //
-// FUSED (one launch per layer, A.t0 = the layer): instead of staging the rows,
-// back them up at once against V of layer t+1 (finished by the previous launch
-// of the stream) and write V, policy of layer t; see fused_backup below.
+// FUSED (k_build_fused, one cooperative launch over all layers): instead of
+// staging the rows, back them up at once against V of layer t+1 (the rows it
+// reads, waited for by wait_rows) and write V, policy of layer t; see
+// fused_backup.
 // Row stride (floats) of the staged coefficients: a lane reads 8-byte pairs
 // of row a + 16r, so an even stride with stride/2 odd (or an odd stride) keeps
 // the 16 rows of a warp's loads on distinct banks.
