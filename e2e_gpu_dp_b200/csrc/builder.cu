@@ -615,18 +615,29 @@ __device__ __forceinline__ void build_tile(const BuildArgs& A, unsigned char* sm
   // once per CTA: the next chunk's copies run while the warps count the
   // current one (each warp loading them from L2: 200x200x120 builder 365 ms,
   // staged: 361 ms).
+  // With two buffers (A.ybufs == 2) chunk c+1 is staged into the other buffer
+  // as soon as every warp is past chunk c-1, which the barrier opening chunk c
+  // shows, so the loop needs that one barrier a chunk; with one buffer a second
+  // barrier after the velocity step frees it for the next chunk.
   const int ys = coeff_stride(nm);
   const float* ylayer = A.F.Y + (int64_t)T * P.nrzns * nm;
+  const bool two_bufs = A.ybufs == 2;
+  const int yalt = two_bufs ? rc * ys : 0;  // offset of the other buffer, toggled by xor
+  int yoff = 0;
   stage_coeffs(ysm, ys, ylayer, min(rc, P.nrzns), nm, tid, nthr);
-  for (int base = 0; base < P.nrzns; base += rc) {
+  for (int base = 0; base < P.nrzns; base += rc, yoff ^= yalt) {
     const int clen = min(rc, P.nrzns - base);
+    float* const ycur = ysm + yoff;
     asm volatile("cp.async.wait_all;" ::: "memory");
     __syncthreads();  // the chunk's coefficients are staged; the previous chunk is consumed
+    if (two_bufs && base + rc < P.nrzns)
+      stage_coeffs(ysm + (yoff ^ yalt), ys, ylayer + (int64_t)(base + rc) * nm, min(rc, P.nrzns - base - rc), nm,
+                   tid, nthr);
     // extract_velocity, src/build_model.cu:389-401: mean + sum over modes, both
     // sums as one chain of packed fused multiply-adds in the reference's order
     if (cvalid) {
       const float2* md = modes + cl;
-      const float* yb = ysm;
+      const float* yb = ycur;
       const int ystep = per * ys;
       int q = a;
       // four of the lane's realisations at a time: each mode pair read from
@@ -694,9 +705,11 @@ __device__ __forceinline__ void build_tile(const BuildArgs& A, unsigned char* sm
         myvel[q] = make_float2(u1 + sum.x, v1 + sum.y);
       }
     }
-    __syncthreads();  // every warp has read the chunk's coefficients
-    if (base + rc < P.nrzns)
-      stage_coeffs(ysm, ys, ylayer + (int64_t)(base + rc) * nm, min(rc, P.nrzns - base - rc), nm, tid, nthr);
+    if (!two_bufs) {
+      __syncthreads();  // every warp has read the chunk's coefficients
+      if (base + rc < P.nrzns)
+        stage_coeffs(ysm, ys, ylayer + (int64_t)(base + rc) * nm, min(rc, P.nrzns - base - rc), nm, tid, nthr);
+    }
     if (mode == MODE_FIXED) {
       for (int q = 0; q < clen; ++q) sumR += r_fixed;
     } else if (mode == MODE_WINDOW) {
@@ -1082,12 +1095,42 @@ int build_lanes_log2(int na) {
   return l;
 }
 
-size_t build_smem_bytes(int na, int nm, int rc, bool unit) {
+size_t build_smem_bytes(int na, int nm, int rc, bool unit, int ybufs) {
   const int nthr = 32 << build_lanes_log2(na);
   return (size_t)2 * nm * 32 * sizeof(float) + (size_t)32 * (rc + 2) * sizeof(float2) +
          (unit ? 0 : (size_t)MASK_COUNT * nthr * sizeof(uint64_t)) +
          (size_t)(kWinBins + 1) * ((size_t)1 << counter_log2_stride(nthr)) * sizeof(uint16_t) +
-         (size_t)rc * coeff_stride(nm) * sizeof(float);
+         (size_t)ybufs * rc * coeff_stride(nm) * sizeof(float);
+}
+
+int build_ctas_per_sm(int na, size_t smem, bool unit) {
+  int dev = 0, smem_sm = 0, reserved = 0, regs_sm = 0, thr_sm = 0;
+  // a failed query answers 0 and leaves no error behind for the next launch check
+  auto none = []() {
+    cudaGetLastError();
+    return 0;
+  };
+  if (cudaGetDevice(&dev) != cudaSuccess) return none();
+  if (cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev) != cudaSuccess ||
+      cudaDeviceGetAttribute(&reserved, cudaDevAttrReservedSharedMemoryPerBlock, dev) != cudaSuccess ||
+      cudaDeviceGetAttribute(&regs_sm, cudaDevAttrMaxRegistersPerMultiprocessor, dev) != cudaSuccess ||
+      cudaDeviceGetAttribute(&thr_sm, cudaDevAttrMaxThreadsPerMultiProcessor, dev) != cudaSuccess)
+    return none();
+  const int nthr = 32 << build_lanes_log2(na);
+  int best = thr_sm / nthr;
+  cudaFuncAttributes fa[2];
+  cudaError_t e = unit ? cudaFuncGetAttributes(&fa[0], k_build_tiles<uint16_t, true>)
+                       : cudaFuncGetAttributes(&fa[0], k_build_tiles<uint16_t, false>);
+  if (e != cudaSuccess) return none();
+  e = unit ? cudaFuncGetAttributes(&fa[1], k_build_fused<uint32_t, true>)
+           : cudaFuncGetAttributes(&fa[1], k_build_fused<uint32_t, false>);
+  if (e != cudaSuccess) return none();
+  for (const cudaFuncAttributes& f : fa) {
+    const size_t per_cta = smem + f.sharedSizeBytes + (size_t)reserved;
+    best = std::min(best, (int)((size_t)smem_sm / per_cta));
+    if (f.numRegs > 0) best = std::min(best, regs_sm / (f.numRegs * nthr));
+  }
+  return best;
 }
 
 // the dynamic shared-memory cap of a kernel only grows: builds on other host
@@ -1110,7 +1153,7 @@ template <typename CntT, bool UNIT>
 static cudaError_t launch_one(const BuildArgs& A, int n_layers, cudaStream_t st) {
   dim3 grid((unsigned)A.tiles_per_layer, (unsigned)n_layers);
   dim3 block((unsigned)(32u << A.lanes_log2));
-  const size_t sm = build_smem_bytes(A.P.na, A.P.nm, A.rc, UNIT);
+  const size_t sm = build_smem_bytes(A.P.na, A.P.nm, A.rc, UNIT, A.ybufs);
   static std::mutex mu;
   static int cap_set[64] = {};
   cudaError_t e = raise_smem_cap(k_build_tiles<CntT, UNIT>, sm, cap_set, mu);
@@ -1123,7 +1166,7 @@ template <bool UNIT>
 static cudaError_t launch_fused(const BuildArgs& A, cudaStream_t st, int* grid_out) {
   auto kern = k_build_fused<uint32_t, UNIT>;
   const int threads = 32 << A.lanes_log2;
-  const size_t sm = build_smem_bytes(A.P.na, A.P.nm, A.rc, UNIT);
+  const size_t sm = build_smem_bytes(A.P.na, A.P.nm, A.rc, UNIT, A.ybufs);
   static std::mutex mu;
   static int cap_set[64] = {};
   cudaError_t e = raise_smem_cap(kern, sm, cap_set, mu);

@@ -693,16 +693,27 @@ e2e_status plan_build(const e2e_problem* p, int count_bits, int64_t stage_hint, 
     unit = std::fabs(xs[1] - xs[0]) == 1.0f && std::fabs(ys[1] - ys[0]) == 1.0f;
   }
   pl->rc = unit ? 128 : 64;
-  size_t sm = build_smem_bytes(pl->na, p->nmodes, pl->rc, unit);
+  size_t sm = build_smem_bytes(pl->na, p->nmodes, pl->rc, unit, 1);
   if (unit && pl->na <= 16 && sm > 112 * 1024) {
     pl->rc = 64;
-    sm = build_smem_bytes(pl->na, p->nmodes, pl->rc, unit);
+    sm = build_smem_bytes(pl->na, p->nmodes, pl->rc, unit, 1);
   }
   while (sm > 200 * 1024 && pl->rc > 16) {
     pl->rc /= 2;
-    sm = build_smem_bytes(pl->na, p->nmodes, pl->rc, unit);
+    sm = build_smem_bytes(pl->na, p->nmodes, pl->rc, unit, 1);
   }
   if (sm > 220 * 1024) return fail(E2E_ERR_UNSUPPORTED, "shared memory need too large (nmodes/actions)");
+  // A second coefficient buffer lets the chunk loop stage chunk c+1 while
+  // chunk c is read, with one CTA barrier a chunk instead of two; taken only
+  // when it costs no builder CTA per SM.
+  pl->ybufs = 1;
+  {
+    const size_t sm2 = build_smem_bytes(pl->na, p->nmodes, pl->rc, unit, 2);
+    if (sm2 <= 220 * 1024) {
+      const int c1 = build_ctas_per_sm(pl->na, sm, unit);
+      if (c1 > 0 && build_ctas_per_sm(pl->na, sm2, unit) >= c1) pl->ybufs = 2;
+    }
+  }
   if (pl->tiles_per_layer > 0x7fffffff || p->nt - 1 > 65535)
     return fail(E2E_ERR_UNSUPPORTED, "grid too large for one launch");
   pl->stage_cap = stage_hint > 0 ? stage_hint : pl->n_rows * 4 + 4096;
@@ -817,6 +828,7 @@ e2e_status run_build(const e2e_problem* p, const FieldsOnDevice& fd, const Build
     A.t0 = 0;
     A.tiles_per_layer = (int)pl.tiles_per_layer;
     A.rc = pl.rc;
+    A.ybufs = pl.ybufs;
     A.lanes_log2 = build_lanes_log2(pl.na);
     A.stage_col = stage_col;
     A.stage_cnt = stage_cnt;

@@ -108,6 +108,7 @@ extern "C" e2e_status e2e_build_solve(const e2e_problem* p, const e2e_fields* f,
     A.F = fd.F;
     A.tiles_per_layer = (int)pl.tiles_per_layer;
     A.rc = pl.rc;
+    A.ybufs = pl.ybufs;
     A.lanes_log2 = build_lanes_log2(pl.na);
     A.counters = ctr;
     A.pool = pool;

@@ -87,6 +87,7 @@ struct BuildPlan {
   int64_t ncells = 0, ns = 0, n_rows = 0, tiles_per_layer = 0, n_tiles = 0;
   int64_t etiles_per_layer = 0, cells_per_tile = 32;  // emission tiles (one per builder warp)
   int na = 0, rc = 128;
+  int ybufs = 1;  // coefficient buffers of the builder's chunk loop (2 when occupancy allows)
   int64_t stage_cap = 0, pool_units = 0;
   bool keep_sums = false;  // keep per-row reward sums (e2e_build_opts.keep_reward_parts)
 };

@@ -30,6 +30,7 @@ struct BuildArgs {
   int t0;               // first layer of this launch (blockIdx.y offset)
   int tiles_per_layer;  // CTAs per layer = ceil(ncells / 32); emission tiles are warps
   int rc;               // realisations per warp-private velocity chunk
+  int ybufs;            // chunk coefficient buffers in shared memory: 1, or 2 (one CTA barrier a chunk)
   int lanes_log2;       // lanes per cell = 1 << lanes_log2 >= na
   int32_t* stage_col;
   void* stage_cnt;
@@ -64,7 +65,11 @@ struct AssembleArgs {
 };
 
 int build_lanes_log2(int na);
-size_t build_smem_bytes(int na, int nm, int rc, bool unit);
+size_t build_smem_bytes(int na, int nm, int rc, bool unit, int ybufs);
+// builder CTAs that fit one SM with this dynamic shared memory (the lower of
+// the staging and the fused kernel), from the kernels' registers and static
+// shared memory and the device's limits
+int build_ctas_per_sm(int na, size_t smem, bool unit);
 cudaError_t launch_build_tiles(const BuildArgs& A, int count_bits, int n_layers, cudaStream_t st);
 // The fused build+backup of every layer (uses A.V, A.pi, A.pool, A.counters,
 // A.layer_done; no staging): one cooperative launch whose CTAs take the tiles
