@@ -168,6 +168,38 @@ __host__ __device__ __forceinline__ int coeff_stride(int nm) {
   return (nm & 1) ? nm : (((nm >> 1) & 1) ? nm : nm + 2);
 }
 
+// Which group of a layer's cells a builder warp takes.  A warp holds cpw
+// consecutive cells (cpw = 32 / warps per CTA); its group index is also its
+// emission tile, so the canonical CSR order does not depend on which CTA ran
+// it.  Warps whose windows can reach the grid's edge run the slower counting
+// loop with the domain clamps; mixed into a CTA of plain warps they keep the
+// plain warps waiting at every chunk barrier.  So the slots of a layer list
+// the groups with a cell within kEdgeBand cells of the border first, then the
+// interior groups, each in index order, and CTA `tile` takes slots
+// tile * nwarps ... + nwarps - 1.  Identity when cpw does not divide g or the
+// grid has no interior.
+static constexpr int kEdgeBand = 7;  // window reach (kWin / 2 + 1) plus a mean-flow drift of two cells
+
+__device__ __forceinline__ int64_t group_of_slot(int64_t s, int g, int cpw) {
+  const int64_t gq = g / cpw, ngroups = (int64_t)g * gq;
+  const int qlo = (kEdgeBand + cpw - 1) / cpw, qhi = (g - kEdgeBand) / cpw - 1;
+  const int ni = qhi - qlo + 1, nri = g - 2 * kEdgeBand;
+  if (g % cpw != 0 || ni <= 0 || nri <= 0 || s >= ngroups) return s;
+  const int64_t ne_row = gq - ni, top = (int64_t)kEdgeBand * gq, mid = (int64_t)nri * ne_row;
+  const int64_t n_edge = 2 * top + mid;
+  if (s >= n_edge) {  // interior: rows [E, g-E), groups [qlo, qhi]
+    const int64_t k = s - n_edge;
+    return (kEdgeBand + k / ni) * gq + qlo + k % ni;
+  }
+  if (s < top) return s;  // rows [0, E)
+  int64_t e = s - top;
+  if (e < mid) {  // the edge groups of an interior row: [0, qlo) and (qhi, gq)
+    const int64_t k = e % ne_row;
+    return (kEdgeBand + e / ne_row) * gq + (k < qlo ? k : k + ni);
+  }
+  return (int64_t)(g - kEdgeBand) * gq + (e - mid);  // rows [g-E, g)
+}
+
 // Stages the coefficients of clen realisations (rows of nm floats from src)
 // in shared memory, rows ys floats apart: 4-byte asynchronous copies, the
 // CTA's threads striding over the elements; one commit group per call.
@@ -275,7 +307,20 @@ __device__ __forceinline__ void build_tile(const BuildArgs& A, unsigned char* sm
   const int g = P.g;
   const int64_t nc = (int64_t)g * g;
   const int64_t c0 = (int64_t)tile * 32;
-  const int64_t cell = c0 + cl;
+  // the cells of the tile's warps' groups (group_of_slot), local cell l at
+  // cell_tab[l]; the fused pass keeps the identity (its completion counts are
+  // per grid row of consecutive cells)
+  __shared__ int cell_tab[32];
+  if (!FUSED) {
+    if (tid < 32) {
+      const int cpw_log2 = 5 - lanes_log2;
+      const int64_t grp = group_of_slot((int64_t)tile * nwarps + (tid >> cpw_log2), g, 1 << cpw_log2);
+      cell_tab[tid] = (int)((grp << cpw_log2) + (tid & ((1 << cpw_log2) - 1)));
+    }
+    __syncthreads();
+  }
+  auto cell_of = [&](int l) -> int64_t { return FUSED ? c0 + l : (int64_t)cell_tab[l]; };
+  const int64_t cell = cell_of(cl);
   const bool valid = (cell < nc) && (a < P.na);
   const int nm = P.nm;
   const int log2S = counter_log2_stride(nthr);
@@ -297,7 +342,7 @@ __device__ __forceinline__ void build_tile(const BuildArgs& A, unsigned char* sm
   // ---- stage the modes of the tile's cells as (ui_k, vi_k) pairs ---------
   for (int idx = tid; idx < 2 * nm * 32; idx += nthr) {
     int k2 = idx >> 5, l = idx & 31;
-    int64_t c = c0 + l;
+    int64_t c = cell_of(l);
     float val = 0.f;
     if (c < nc) {
       val = (k2 < nm) ? __ldg(A.F.ui + ((int64_t)T * nm + k2) * nc + c)
@@ -354,7 +399,7 @@ __device__ __forceinline__ void build_tile(const BuildArgs& A, unsigned char* sm
         bool hit = false;
         if (idx < s1) {
           const int c = idx / kNbBits, ob = idx - c * kNbBits;
-          const int64_t cc = c0 + c;
+          const int64_t cc = cell_of(c);
           const int da = ob / kNbSide - kNb, db = ob % kNbSide - kNb;
           if (cc < nc && !(da == 0 && db == 0)) {
             const int ci1 = (int)(cc / g), cj1 = (int)(cc - (int64_t)ci1 * g);
@@ -376,7 +421,7 @@ __device__ __forceinline__ void build_tile(const BuildArgs& A, unsigned char* sm
       for (int pi = warp; pi < n; pi += nwarps) {
         const int idx = pairs[pi];
         const int c = idx / kNbBits, ob = idx - c * kNbBits;
-        const int64_t cc = c0 + c;
+        const int64_t cc = cell_of(c);
         const int da = ob / kNbSide - kNb, db = ob % kNbSide - kNb;
         const int ci1 = (int)(cc / g), cj1 = (int)(cc - (int64_t)ci1 * g);
         const int oi = ci1 + da, oj = cj1 + db;
@@ -895,14 +940,17 @@ __device__ __forceinline__ void build_tile(const BuildArgs& A, unsigned char* sm
   unsigned long long wbase = 0;
   if (lane == 0) {
     wbase = atomicAdd(A.counters + CTR_STAGE, (unsigned long long)total);
-    const int64_t wt = ((int64_t)T * A.tiles_per_layer + tile) * nwarps + warp;
+    const int64_t wt = (int64_t)T * A.tiles_per_layer * nwarps + (cell_tab[warp << (5 - A.lanes_log2)] >> (5 - A.lanes_log2));
     A.tile_base[wt] = (int64_t)wbase;
     A.tile_len[wt] = total;
   }
   wbase = __shfl_sync(0xffffffffu, wbase, 0);
   if (!valid) return;
   const int excl = incl - nnz;
-  const int64_t grow = ((int64_t)T * nc + cell) * P.na + a;
+  // the lane's cell again from the group table (a shared-memory load, not a
+  // register held through the sample loops)
+  const int64_t cell_e = cell_of(cl);
+  const int64_t grow = ((int64_t)T * nc + cell_e) * P.na + a;
   A.row_off[grow] = (uint32_t)excl;
   A.R[grow] = sumR / P.nrzns;  // compute_mean, src/build_model.cu:567
   if (A.sumR) A.sumR[grow] = sumR;  // kept for re-targeting (served requests)
@@ -912,7 +960,7 @@ __device__ __forceinline__ void build_tile(const BuildArgs& A, unsigned char* sm
   CntT* scnt = reinterpret_cast<CntT*>(A.stage_cnt);
   const int64_t next_layer = (int64_t)(T + 1) * nc;
   if (mode == MODE_FIXED) {
-    A.stage_col[off] = (int32_t)(next_layer + cell);
+    A.stage_col[off] = (int32_t)(next_layer + cell_e);
     scnt[off] = (CntT)P.nrzns;
   } else if (mode == MODE_WINDOW) {
     for (int wl = 0; wl < kWinBins; ++wl) {
