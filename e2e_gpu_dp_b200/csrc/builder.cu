@@ -8,19 +8,26 @@
 //   reduce_kernel            :597-644  (one thread walks 441 bins per cell)
 // with one kernel over all layers:
 //
-//  * a CTA owns a tile of 32 consecutive cells of one layer and all actions
-//    (warp w = action w, lane = cell), i.e. a contiguous range of model rows;
-//  * the velocity of every (cell, realisation) is computed once per CTA chunk
-//    (u + sum_k ui_k*Y_k, reference order) into shared memory and reused by all
-//    actions (the reference recomputes it per action);
-//  * each (cell, action) row histogram lives in a thread-private 7x7 window of
+//  * a CTA owns 32 cells of one layer and all actions; a warp holds 32/P
+//    consecutive cells x P action lanes (P = next power of two >= actions),
+//    i.e. a contiguous range of model rows.  Which cell groups a CTA takes is
+//    chosen by group_of_slot (warps that reach the grid edge in CTAs of their
+//    own); the fused build+backup keeps 32 consecutive cells;
+//  * the velocity of every (cell, realisation) is computed once per chunk of
+//    realisations (u + sum_k ui_k*Y_k, reference order) into warp-private
+//    shared memory and reused by all actions (the reference recomputes it per
+//    action); the chunk's mode coefficients are staged once per CTA with
+//    asynchronous copies, double-buffered when shared memory allows;
+//  * each (cell, action) row histogram lives in a thread-private 8x8 window of
 //    16-bit counters in shared memory, placed around the landing cell of the
-//    mean flow - no atomics, no sort, exact integer counts.  A sample outside
-//    the window but inside the reference's m x m neighbourhood switches that
-//    row to a dense m*m histogram taken from a global pool (rare);
+//    mean flow - no atomics, no sort, exact integer counts.  Samples outside
+//    the window are re-run through the full expression; a sample inside the
+//    reference's m x m neighbourhood but outside the window switches that row
+//    to a dense m*m histogram taken from a global pool (rare);
 //  * per-row nonzero bins are emitted in bin order (ascending next state, the
-//    order of reduce_kernel) into a staging area at a tile offset obtained with
-//    one atomicAdd per CTA, with the row's tile-relative offset and R = sumR/nrzns;
+//    order of reduce_kernel) into a staging area at an offset obtained with
+//    one atomicAdd per warp (the warp's emission tile = its cell group), with
+//    the row's tile-relative offset and R = sumR/nrzns;
 //  * K2 scans the tile lengths, K3 moves every tile into canonical CSR order and
 //    writes row_ptr.
 #include <algorithm>
