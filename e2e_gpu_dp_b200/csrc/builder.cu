@@ -143,13 +143,13 @@ __device__ __forceinline__ void fused_backup(const BuildArgs& A, int T, int64_t 
 
 // K1.  Template: CntT = staged count type; UNIT = unit cell spacing.
 //
-// A CTA owns 32 consecutive cells of one layer and all their actions.  Warp w
-// holds cells_per_warp = 32/P cells (P = next power of two >= Na) and lane
-// (c, a) is the row (cell c, action a), so a warp computes the velocities of
-// its own cells (u + sum_k ui_k*Y_k, reference order) into warp-private
-// shared memory from the chunk's coefficients (staged once per CTA between two
-// barriers a chunk), samples without further CTA barriers and emits its own
-// rows.
+// A CTA owns 32 cells of one layer and all their actions.  Warp w holds
+// cells_per_warp = 32/P consecutive cells (P = next power of two >= Na; which
+// group, group_of_slot) and lane (c, a) is the row (cell c, action a), so a
+// warp computes the velocities of its own cells (u + sum_k ui_k*Y_k, reference
+// order) into warp-private shared memory from the chunk's coefficients (staged
+// once per CTA; one barrier a chunk with two buffers, two with one), samples
+// without further CTA barriers and emits its own rows.
 //
 // Per row the 8x8 window of the grid around the mean-flow landing cell is
 // classified once.  The obstacle override is bit 15 of the bin's 16-bit
