@@ -175,6 +175,19 @@ __host__ __device__ __forceinline__ int coeff_stride(int nm) {
   return (nm & 1) ? nm : (((nm >> 1) & 1) ? nm : nm + 2);
 }
 
+// min / max that return NaN when either input is NaN (min.NaN / max.NaN):
+// a chunk's velocity bounds then become NaN if any velocity is.
+__device__ __forceinline__ float fmin_nan(float a, float b) {
+  float r;
+  asm("min.NaN.f32 %0, %1, %2;" : "=f"(r) : "f"(a), "f"(b));
+  return r;
+}
+__device__ __forceinline__ float fmax_nan(float a, float b) {
+  float r;
+  asm("max.NaN.f32 %0, %1, %2;" : "=f"(r) : "f"(a), "f"(b));
+  return r;
+}
+
 // Which group of a layer's cells a builder warp takes.  A warp holds cpw
 // consecutive cells (cpw = 32 / warps per CTA); its group index is also its
 // emission tile, so the canonical CSR order does not depend on which CTA ran
@@ -675,6 +688,8 @@ __device__ __forceinline__ void build_tile(const BuildArgs& A, unsigned char* sm
   const float* ylayer = A.F.Y + (int64_t)T * P.nrzns * nm;
   const bool two_bufs = A.ybufs == 2;
   const int yalt = two_bufs ? rc * ys : 0;  // offset of the other buffer, toggled by xor
+  // velocity bounds of the chunk (plain warps of the unit-spacing staging kernel)
+  const bool track = UNIT && !FUSED && !clamp_warp && P.dt > 0.f;
   int yoff = 0;
   stage_coeffs(ysm, ys, ylayer, min(rc, P.nrzns), nm, tid, nthr);
   for (int base = 0; base < P.nrzns; base += rc, yoff ^= yalt) {
@@ -685,6 +700,8 @@ __device__ __forceinline__ void build_tile(const BuildArgs& A, unsigned char* sm
     if (two_bufs && base + rc < P.nrzns)
       stage_coeffs(ysm + (yoff ^ yalt), ys, ylayer + (int64_t)(base + rc) * nm, min(rc, P.nrzns - base - rc), nm,
                    tid, nthr);
+    float2 vlo = make_float2(__int_as_float(0x7f800000), __int_as_float(0x7f800000));  // +inf
+    float2 vhi = make_float2(__int_as_float(0xff800000), __int_as_float(0xff800000));  // -inf
     // extract_velocity, src/build_model.cu:389-401: mean + sum over modes, both
     // sums as one chain of packed fused multiply-adds in the reference's order
     if (cvalid) {
@@ -734,10 +751,18 @@ __device__ __forceinline__ void build_tile(const BuildArgs& A, unsigned char* sm
             s3 = __ffma2_rn(m0, make_float2(c3, c3), s3);
           }
         }
-        myvel[q] = make_float2(u1 + s0.x, v1 + s0.y);
-        myvel[q + per] = make_float2(u1 + s1.x, v1 + s1.y);
-        myvel[q + 2 * per] = make_float2(u1 + s2.x, v1 + s2.y);
-        myvel[q + 3 * per] = make_float2(u1 + s3.x, v1 + s3.y);
+        const float2 w0 = make_float2(u1 + s0.x, v1 + s0.y), w1 = make_float2(u1 + s1.x, v1 + s1.y);
+        const float2 w2 = make_float2(u1 + s2.x, v1 + s2.y), w3 = make_float2(u1 + s3.x, v1 + s3.y);
+        myvel[q] = w0;
+        myvel[q + per] = w1;
+        myvel[q + 2 * per] = w2;
+        myvel[q + 3 * per] = w3;
+        if (track) {
+          vlo.x = fmin_nan(vlo.x, fmin_nan(fmin_nan(w0.x, w1.x), fmin_nan(w2.x, w3.x)));
+          vlo.y = fmin_nan(vlo.y, fmin_nan(fmin_nan(w0.y, w1.y), fmin_nan(w2.y, w3.y)));
+          vhi.x = fmax_nan(vhi.x, fmax_nan(fmax_nan(w0.x, w1.x), fmax_nan(w2.x, w3.x)));
+          vhi.y = fmax_nan(vhi.y, fmax_nan(fmax_nan(w0.y, w1.y), fmax_nan(w2.y, w3.y)));
+        }
       }
       for (; q < clen; q += per) {
         const float* y = yb + q * ys;
@@ -754,8 +779,44 @@ __device__ __forceinline__ void build_tile(const BuildArgs& A, unsigned char* sm
             sum = __ffma2_rn(md[k * 32], make_float2(yk, yk), sum);
           }
         }
-        myvel[q] = make_float2(u1 + sum.x, v1 + sum.y);
+        const float2 w0 = make_float2(u1 + sum.x, v1 + sum.y);
+        myvel[q] = w0;
+        if (track) {
+          vlo = make_float2(fmin_nan(vlo.x, w0.x), fmin_nan(vlo.y, w0.y));
+          vhi = make_float2(fmax_nan(vhi.x, w0.x), fmax_nan(vhi.y, w0.y));
+        }
       }
+    }
+    // Plain warps of the staging kernel: does every sample of the chunk land in
+    // its row's window?  The snapping chain (advection, offset, two round-down
+    // adds) is monotone in each velocity component (every step rounds a
+    // function increasing in the component, x increasing and y decreasing, for
+    // dt > 0), so the bins of the chunk's samples lie between those of the
+    // bounding box's corners (vx min, vy max) and (vx max, vy min) of the cell's
+    // velocities (a NaN velocity makes the bounds NaN: never in the window).
+    // If the corners are in the window for every counting lane of the warp,
+    // the chunk runs the loop without the window test and the miss counter.
+    bool in_win = false;
+    if (track) {
+      for (int o = 1; o < per; o <<= 1) {
+        vlo.x = fmin_nan(vlo.x, __shfl_xor_sync(0xffffffffu, vlo.x, o));
+        vlo.y = fmin_nan(vlo.y, __shfl_xor_sync(0xffffffffu, vlo.y, o));
+        vhi.x = fmax_nan(vhi.x, __shfl_xor_sync(0xffffffffu, vhi.x, o));
+        vhi.y = fmax_nan(vhi.y, __shfl_xor_sync(0xffffffffu, vhi.y, o));
+      }
+      bool ok = true;
+      if (mode == MODE_WINDOW) {
+        const uint32_t M = 0x4B400000u;
+        const float2 magic = make_float2(12582912.0f - (float)wj0, 12582912.0f - (float)wi0);
+        const float2 half = make_float2(0.5f, 0.5f);
+        const float2 tl = __fadd2_rd(
+            __fadd2_rd(__ffma2_rn(advect2(FF, csn, make_float2(vlo.x, vhi.y), dt2, xy1), sgn, org), half), magic);
+        const float2 th = __fadd2_rd(
+            __fadd2_rd(__ffma2_rn(advect2(FF, csn, make_float2(vhi.x, vlo.y), dt2, xy1), sgn, org), half), magic);
+        ok = ((__float_as_uint(tl.x) ^ M) | (__float_as_uint(tl.y) ^ M) | (__float_as_uint(th.x) ^ M) |
+              (__float_as_uint(th.y) ^ M)) < (uint32_t)kWin;
+      }
+      in_win = __all_sync(0xffffffffu, ok);
     }
     if (!two_bufs) {
       __syncthreads();  // every warp has read the chunk's coefficients
@@ -826,6 +887,31 @@ __device__ __forceinline__ void build_tile(const BuildArgs& A, unsigned char* sm
           // the pairs below and 419 ms without them (200x200x120)
 #pragma unroll 16
           for (int q = 0; q < clen; ++q) count_sample(myvel[q]);
+        } else if (in_win) {
+          // every sample of the chunk is in the window (bounding box above): the
+          // bin is the low six bits of (by << 3) + bx (the 0x4B400000 offsets
+          // have none), masked so that the address stays in the lane's counters
+          const uint32_t wsh = (uint32_t)__cvta_generic_to_shared(wcol);
+          const uint32_t row_bytes = 1u << sh;
+          auto count_in_window = [&](float2 vv) {
+            const float2 xy = advect2(FF, csn, vv, dt2, xy1);
+            const float2 w = __fadd2_rd(__ffma2_rn(xy, sgn, org), make_float2(0.5f, 0.5f));
+            const float2 t = __fadd2_rd(w, magic);
+            const uint32_t b = ((__float_as_uint(t.y) << 3) + __float_as_uint(t.x)) & 63u;
+            const uint32_t addr = wsh + b * row_bytes;
+            unsigned short v;
+            asm volatile("ld.shared.u16 %0, [%1];" : "=h"(v) : "r"(addr));
+            const unsigned short v1 = (unsigned short)(v + 1);
+            asm volatile("st.shared.u16 [%0], %1;" ::"r"(addr), "h"(v1));
+          };
+          int q = 0;
+#pragma unroll 8
+          for (; q + 1 < clen; q += 2) {
+            const float4 v2 = *reinterpret_cast<const float4*>(myvel + q);
+            count_in_window(make_float2(v2.x, v2.y));
+            count_in_window(make_float2(v2.z, v2.w));
+          }
+          if (q < clen) count_in_window(myvel[q]);
         } else {
           // two realisations a 16-byte load (the velocity rows have an even
           // stride): 200x200x120 builder 409 -> 393 ms
