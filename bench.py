@@ -231,6 +231,15 @@ def workload_config(prob, ws: int = 1) -> dict:
     }
 
 
+def assembly_bytes(nnz: int, n_rows: int, count_bytes: int, index_bits: int) -> int:
+    """Bytes the CSR assembly (K2 scan of the tile lengths, K3 copy) must move:
+    the staged entries read and the canonical entries written (nnz*(4 +
+    b_cnt) each way), the per-row offsets read and the row pointers written
+    (4 or 8 bytes)."""
+    ptr = 8 if index_bits == 64 else 4
+    return int(2 * nnz * (4 + count_bytes) + n_rows * 4 + (n_rows + 1) * ptr)
+
+
 def vi_bytes_per_iteration(ns: int, na: int, nnz: int, count_bytes: int) -> int:
     """Algorithmic bytes of one VI sweep over the CSR with a per-state row
     pointer: nnz*(b_cnt + 4) + (Ns + 1)*4 + Na*Ns*4 + 3*Ns*4 (entries, row
@@ -571,6 +580,12 @@ def run_ours(args, ws, rank, local):
                 "hbm": hbm_part}
     else:
         roof = {"kernel": "k_build_tiles", "bound": "hbm", **hbm_part}
+    asm_bytes = assembly_bytes(info["nnz"], info["n_rows"], cb, info["index_bits"])
+    asm_gbs = asm_bytes / (asm_ms * 1e-3) / 1e9 if asm_ms > 0 else None
+    asm_roof = {"kernels": "k_scan_* (K2) + k_assemble (K3)", "bound": "hbm", "ms": round(asm_ms, 3),
+                "algorithmic_bytes": asm_bytes,
+                "achieved": round(asm_gbs, 1) if asm_gbs else None, "peak": hbm, "unit": "GB/s",
+                "frac": round(asm_gbs / hbm, 4) if asm_gbs else None}
     line = {
         "metric": "build+VI sec",
         "value": round(value_s, 6),
@@ -601,6 +616,7 @@ def run_ours(args, ws, rank, local):
                       "pack": round(pack_ms, 3), "solve": round(solve_ms, 3),
                       "layered_pass": round(pass_ms, 3)},
         "roofline": roof,
+        "assembly": asm_roof,
         "build_samples_per_s": round(samples / (k1_ms * 1e-3), 1),
         "vi": {"kernel": "k_vi_chunks (Jacobi, reference schedule)", "iterations": jst["iterations"],
                "algorithmic_bytes_per_sweep": vi_bytes,

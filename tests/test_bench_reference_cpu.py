@@ -77,6 +77,12 @@ def test_vi_bytes_and_issue_roofline():
     assert abs(r["achieved"] - r["warp_inst_per_sample"] * 32e9) < 1e-3
 
 
+def test_assembly_bytes():
+    # entries read and written, row offsets read, row pointers written
+    assert bench.assembly_bytes(100, 10, 2, 32) == 2 * 100 * 6 + 10 * 4 + 11 * 4
+    assert bench.assembly_bytes(100, 10, 4, 64) == 2 * 100 * 8 + 10 * 4 + 11 * 8
+
+
 def test_parity_sample_counts_each_row_once():
     """A row one entry longer on the device is one mismatched row; the rows
     after it still compare equal."""
