@@ -764,7 +764,7 @@ def run_batched(n_models: int = 256, seed: int = 2024) -> dict:
     }
 
 
-def run_served(rates=(50, 200, 500, 1000, 2000), seconds_per_rate=10.0, max_requests=20000,
+def run_served(rates=(50, 100, 200, 500, 1000, 2000), seconds_per_rate=10.0, max_requests=20000,
                plain_sample=40) -> dict:
     """Served form: 16 resident fields (15 size classes drawn like the batched
     form plus one 300x300x150 class), Poisson request streams (each request picks
