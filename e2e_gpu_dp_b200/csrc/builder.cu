@@ -1228,12 +1228,16 @@ int build_ctas_per_sm(int na, size_t smem, bool unit) {
     return none();
   const int nthr = 32 << build_lanes_log2(na);
   int best = thr_sm / nthr;
-  cudaFuncAttributes fa[2];
+  // the staging kernel with 16- and 32-bit counts, and the fused kernel
+  cudaFuncAttributes fa[3];
   cudaError_t e = unit ? cudaFuncGetAttributes(&fa[0], k_build_tiles<uint16_t, true>)
                        : cudaFuncGetAttributes(&fa[0], k_build_tiles<uint16_t, false>);
   if (e != cudaSuccess) return none();
-  e = unit ? cudaFuncGetAttributes(&fa[1], k_build_fused<uint32_t, true>)
-           : cudaFuncGetAttributes(&fa[1], k_build_fused<uint32_t, false>);
+  e = unit ? cudaFuncGetAttributes(&fa[1], k_build_tiles<uint32_t, true>)
+           : cudaFuncGetAttributes(&fa[1], k_build_tiles<uint32_t, false>);
+  if (e != cudaSuccess) return none();
+  e = unit ? cudaFuncGetAttributes(&fa[2], k_build_fused<uint32_t, true>)
+           : cudaFuncGetAttributes(&fa[2], k_build_fused<uint32_t, false>);
   if (e != cudaSuccess) return none();
   for (const cudaFuncAttributes& f : fa) {
     const size_t per_cta = smem + f.sharedSizeBytes + (size_t)reserved;

@@ -66,9 +66,9 @@ struct AssembleArgs {
 
 int build_lanes_log2(int na);
 size_t build_smem_bytes(int na, int nm, int rc, bool unit, int ybufs);
-// builder CTAs that fit one SM with this dynamic shared memory (the lower of
-// the staging and the fused kernel), from the kernels' registers and static
-// shared memory and the device's limits
+// builder CTAs that fit one SM with this dynamic shared memory (the lowest of
+// the staging kernels, 16- and 32-bit counts, and the fused kernel), from the
+// kernels' registers and static shared memory and the device's limits
 int build_ctas_per_sm(int na, size_t smem, bool unit);
 cudaError_t launch_build_tiles(const BuildArgs& A, int count_bits, int n_layers, cudaStream_t st);
 // The fused build+backup of every layer (uses A.V, A.pi, A.pool, A.counters,
