@@ -937,6 +937,79 @@ def run_envgen() -> dict:
     return res
 
 
+def small_case_cpu(threads: int, trig=None):
+    """The CPU-runnable workload in full on the host: the 50x50 grid, nt=30,
+    8 headings, 500 realisations, 4 modes, 5 % obstacles, target (45, 25),
+    built by the oracle port (the C restatement of the reference's builder)
+    and solved by its FP64 backward induction, both timed on ``threads``
+    threads.  Returns the timing, the problem, its fields, the oracle's model
+    and its FP64 values."""
+    from e2e_gpu_dp_b200.problem import config, make_fields
+    from oracle import pyoracle as O
+
+    prob, spec = config("c1", seed=1234)
+    fields = make_fields(prob, spec)
+    t0 = time.perf_counter()
+    m = O.build_model(prob, fields, trig=trig, nthreads=threads)
+    t1 = time.perf_counter()
+    V64, _, _ = O.vi_f64_layers(prob.ncells, prob.nt, prob.num_actions, m["row_ptr"], m["col"], m["cnt"],
+                                prob.nrzns, m["R_full"], nthreads=threads)
+    t2 = time.perf_counter()
+    return {"build_s": t1 - t0, "solve_s": t2 - t1, "threads": threads}, prob, fields, m, V64
+
+
+def run_small_case(reps: int = 5) -> dict:
+    """The CPU-runnable workload (50x50, nt=30, 8 headings, 500
+    realisations): the oracle port on all host threads, in full, against the
+    device's build + layered solve of the same seeded inputs (CUDA events,
+    fields resident, after one warm-up), with the device's rows compared to
+    the oracle's bit for bit and its values to the FP64 induction."""
+    import torch
+
+    from e2e_gpu_dp_b200 import api
+
+    from e2e_gpu_dp_b200.problem import config
+
+    threads = os.cpu_count() or 1
+    # the oracle takes the device's cos/sin of the headings, so that the rows
+    # can be compared bit for bit
+    tab = api.action_table(config("c1", seed=1234)[0])
+    cpu, prob, fields, om, V64 = small_case_cpu(threads, trig=(tab["cos"], tab["sin"]))
+    stream = torch.cuda.current_stream()
+    dev = {k: torch.from_numpy(np.ascontiguousarray(v)).cuda() for k, v in fields.items()}
+    V = torch.empty(prob.ns, dtype=torch.float32, device="cuda")
+    pi = torch.empty(prob.ns, dtype=torch.int32, device="cuda")
+    m = api.build_model(prob, dev, stream=stream)
+    m.solve(method="layered", value=V, policy=pi, stream=stream)
+    m.free()
+    torch.cuda.synchronize()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record(stream)
+    for _ in range(reps):
+        m = api.build_model(prob, dev, stream=stream)
+        m.solve(method="layered", value=V, policy=pi, stream=stream)
+        if _ < reps - 1:
+            m.free()
+    b.record(stream)
+    torch.cuda.synchronize()
+    gpu_s = a.elapsed_time(b) / 1e3 / reps
+    h = m.to_host()
+    m.free()
+    same = (np.array_equal(h["row_ptr"], om["row_ptr"]) and np.array_equal(h["col"], om["col"])
+            and np.array_equal(h["cnt"], om["cnt"]))
+    Vh = V.cpu().numpy().astype(np.float64)
+    scale = float(np.max(np.abs(V64)))
+    cpu_s = cpu["build_s"] + cpu["solve_s"]
+    return {"workload": "50x50 grid, nt=30, 8 headings, nrzns 500, 4 modes, 5% obstacles, target (45, 25)",
+            "gpu_build_solve_s": round(gpu_s, 6), "gpu_reps": reps,
+            "cpu_port_s": round(cpu_s, 3), "cpu_port_build_s": round(cpu["build_s"], 3),
+            "cpu_port_solve_s": round(cpu["solve_s"], 3), "cpu_threads": threads,
+            "cpu_kind": "oracle port (C restatement of the reference's builder, FP64 induction), in full",
+            "speedup_vs_cpu": round(cpu_s / gpu_s, 1) if gpu_s > 0 else None,
+            "rows_identical_to_oracle": bool(same),
+            "max_rel_value_err_vs_fp64": float(np.max(np.abs(Vh - V64)) / scale) if scale > 0 else None}
+
+
 def run_precision(sample_rows: int = 80000) -> dict:
     """Precision form: 300x300 grid, nt=150 (13.5 M states), 16 headings,
     nrzns 2000, 8 modes; uint16 counts with int32 next states, FP32 values, the
@@ -1147,6 +1220,8 @@ def main():
     ap.add_argument("--no-served", action="store_true", help="skip the served form")
     ap.add_argument("--envgen-only", action="store_true", help="only the environment generator")
     ap.add_argument("--no-envgen", action="store_true", help="skip the environment generator")
+    ap.add_argument("--no-small-case", action="store_true",
+                    help="skip the 50x50 CPU-runnable workload (oracle port in full vs the device)")
     args = ap.parse_args()
     if args.profile_case:
         return profile_case()
@@ -1188,6 +1263,11 @@ def main():
             line["precision"] = run_precision()
         if rank == 0 and ws == 1 and not args.no_envgen:
             line["envgen"] = run_envgen()
+        if rank == 0 and ws == 1 and not args.no_cpu_baseline and not args.no_small_case:
+            try:
+                line["small_case"] = run_small_case()
+            except Exception as e:  # an auxiliary figure never costs the bench line
+                line["small_case"] = {"error": repr(e)[:300]}
         if rank == 0:
             print(json.dumps(line), flush=True)
     finally:

@@ -2,7 +2,10 @@
 reference programs are replaced by a stand-in that returns their timings: every
 key the line needs is computed (a name error there would cost the whole arm)."""
 import json
+import os
 import types
+
+import numpy as np
 
 import bench
 from oracle import run_ref
@@ -102,3 +105,13 @@ def test_parity_sample_counts_each_row_once():
     rp[r0 + 11:] += 1
     h = {"row_ptr": rp, "col": col, "cnt": cnt, "R": full["R_full"]}
     assert bench.parity_sample(h, [(r0, blk)])["mismatched_rows"] == 1
+
+
+def test_small_case_cpu_leg():
+    """The host half of the 50x50 leg: the oracle builds and solves the whole
+    workload (a failure there would only show on the GPU box)."""
+    cpu, prob, fields, m, V64 = bench.small_case_cpu(threads=max(1, min(8, os.cpu_count() or 1)))
+    assert prob.gsize == 50 and prob.nt == 30 and prob.num_actions == 8 and prob.nrzns == 500
+    assert cpu["build_s"] > 0 and cpu["solve_s"] > 0
+    assert len(m["row_ptr"]) == (prob.nt - 1) * prob.ncells * prob.num_actions + 1
+    assert len(V64) == prob.ns and np.all(np.isfinite(V64))
